@@ -1,0 +1,358 @@
+// FP32 SIMT (FFMA) SGEMM for sm_100a.
+//
+// Replaces the HammerBench device kernel (apps/sgemm/kernel.cpp:279-333).
+// The reference gives each tile of a 16x8 tile group 16x16 output blocks
+// round-robin (kernel.cpp:300-302), streams 16x16 blocks of A and B from DRAM
+// into scratchpad (load_block, kernel.cpp:36-109) and runs a 4x4
+// register-blocked fmaf chain over k (compute_block, kernel.cpp:186-275).
+// Here one CTA owns a BM x BN output tile; A and B tiles stream from HBM into
+// a STAGES-deep shared-memory ring with 16-byte cp.async (zero-filled at the
+// matrix edges), and each thread owns a TM x TN register block that it
+// updates with one fused multiply-add per k in ascending k. The arithmetic
+// per output element is therefore exactly the reference device kernel's:
+// acc = 0.0f; for k = 0..K-1: acc = fmaf(a[m][k], b[k][n], acc).
+//
+// Layout in shared memory (per stage):
+//   A: BM rows x (BK + 4) floats, k contiguous. The +4 pad makes 8
+//      consecutive rows fall in 8 distinct 16-byte bank groups, so the
+//      8 distinct rows read by a quarter-warp with LDS.128 are conflict-free.
+//   B: BK rows x BN floats, n contiguous.
+// Thread layout inside a warp: lane = tn*8 + tm (tm < 8, tn < 4). Thread
+// (tm, tn) owns rows {tm + 8i} and columns {16j + 4tn + c} of its warp tile:
+// a quarter-warp reads 8 distinct A rows (no conflict) and one B float4
+// (broadcast); the whole warp reads 64 contiguous bytes of B.
+#include "common.cuh"
+#include "internal.h"
+
+namespace hbsg {
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+struct FfmaShape {
+  static constexpr int kWarpsM = BM / WM;
+  static constexpr int kWarpsN = BN / WN;
+  static constexpr int kThreads = kWarpsM * kWarpsN * 32;
+  static constexpr int TM = WM / 8;
+  static constexpr int TN = WN / 4;
+  static constexpr int AS = BK + 4;
+  static constexpr int kAStage = BM * AS;
+  static constexpr int kBStage = BK * BN;
+  static constexpr int kSmemBytes = STAGES * (kAStage + kBStage) * 4;
+  static_assert(WM % 8 == 0 && WN % 16 == 0, "warp tile");
+  static_assert(BK % 4 == 0, "BK");
+  static_assert(((AS / 4) & 1) == 1, "A pad keeps 8 rows in distinct bank groups");
+};
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC>
+__global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
+    ffma_sgemm_kernel(FfmaParams p) {
+  using S = FfmaShape<BM, BN, BK, WM, WN, STAGES>;
+  constexpr int NT = S::kThreads;
+  constexpr int TM = S::TM;
+  constexpr int TN = S::TN;
+  constexpr int AS = S::AS;
+
+  extern __shared__ __align__(16) float smem[];
+  float* As = smem;
+  float* Bs = smem + STAGES * S::kAStage;
+
+  // Rasterised tile order: groups of `raster` tile rows, column-major inside
+  // a group, so CTAs resident at the same time share A and B strips in L2.
+  const int t = blockIdx.x;
+  const int group_span = p.raster * p.tiles_n;
+  const int group = t / group_span;
+  const int first_m = group * p.raster;
+  const int gm = min(p.raster, p.tiles_m - first_m);
+  const int in_group = t - group * group_span;
+  const int tile_m = first_m + in_group % gm;
+  const int tile_n = in_group / gm;
+  const int m0 = tile_m * BM;
+  const int n0 = tile_n * BN;
+
+  const int batch = blockIdx.z;
+  const int split = blockIdx.y;
+  const float* __restrict__ A = p.A + batch * p.strideA;
+  const float* __restrict__ B = p.B + batch * p.strideB;
+
+  const int k_begin = split * p.k_per_split;
+  const int k_end = min(p.K, k_begin + p.k_per_split);
+  const int KT = k_end > k_begin ? (k_end - k_begin + BK - 1) / BK : 0;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = warp / S::kWarpsN;
+  const int wn = warp % S::kWarpsN;
+  const int tm = lane & 7;
+  const int tn = lane >> 3;
+
+  auto load_tile = [&](int slot, int kt) {
+    const int k0 = k_begin + kt * BK;
+    float* as = As + slot * S::kAStage;
+    float* bs = Bs + slot * S::kBStage;
+    if constexpr (VEC) {
+      constexpr int ACH = BM * BK / 4;
+#pragma unroll
+      for (int c = tid; c < ACH; c += NT) {
+        const int r = c / (BK / 4);
+        const int kc = (c % (BK / 4)) * 4;
+        const int gr = m0 + r;
+        const int gk = k0 + kc;
+        int bytes = 0;
+        const float* src = A;
+        if (gr < p.M && gk < k_end) {
+          bytes = min(4, k_end - gk) * 4;
+          src = A + (long)gr * p.lda + gk;
+        }
+        cp_async16(as + r * AS + kc, src, bytes);
+      }
+      constexpr int BCH = BK * BN / 4;
+#pragma unroll
+      for (int c = tid; c < BCH; c += NT) {
+        const int r = c / (BN / 4);
+        const int nc = (c % (BN / 4)) * 4;
+        const int gk = k0 + r;
+        const int gn = n0 + nc;
+        int bytes = 0;
+        const float* src = B;
+        if (gk < k_end && gn < p.N) {
+          bytes = min(4, p.N - gn) * 4;
+          src = B + (long)gk * p.ldb + gn;
+        }
+        cp_async16(bs + r * BN + nc, src, bytes);
+      }
+    } else {
+#pragma unroll 4
+      for (int c = tid; c < BM * BK; c += NT) {
+        const int r = c / BK;
+        const int kc = c % BK;
+        const int gr = m0 + r;
+        const int gk = k0 + kc;
+        const bool ok = gr < p.M && gk < k_end;
+        cp_async4(as + r * AS + kc, ok ? A + (long)gr * p.lda + gk : A, ok ? 4 : 0);
+      }
+#pragma unroll 4
+      for (int c = tid; c < BK * BN; c += NT) {
+        const int r = c / BN;
+        const int nc = c % BN;
+        const int gk = k0 + r;
+        const int gn = n0 + nc;
+        const bool ok = gk < k_end && gn < p.N;
+        cp_async4(bs + r * BN + nc, ok ? B + (long)gk * p.ldb + gn : B, ok ? 4 : 0);
+      }
+    }
+  };
+
+  float acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + STAGES - 1;
+      if (nk < KT) load_tile(nk % STAGES, nk);
+      cp_async_commit();
+    }
+    const int slot = kt % STAGES;
+    const float* a_s = As + slot * S::kAStage + (wm * WM + tm) * AS;
+    const float* b_s = Bs + slot * S::kBStage + wn * WN + 4 * tn;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      float4 a4[TM];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) a4[i] = *reinterpret_cast<const float4*>(a_s + i * 8 * AS + kk);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float4 b4[TN / 4];
+#pragma unroll
+        for (int j = 0; j < TN / 4; ++j)
+          b4[j] = *reinterpret_cast<const float4*>(b_s + (kk + k) * BN + 16 * j);
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+          const float av = k == 0 ? a4[i].x : k == 1 ? a4[i].y : k == 2 ? a4[i].z : a4[i].w;
+#pragma unroll
+          for (int j = 0; j < TN / 4; ++j) {
+            acc[i][4 * j + 0] = __fmaf_rn(av, b4[j].x, acc[i][4 * j + 0]);
+            acc[i][4 * j + 1] = __fmaf_rn(av, b4[j].y, acc[i][4 * j + 1]);
+            acc[i][4 * j + 2] = __fmaf_rn(av, b4[j].z, acc[i][4 * j + 2]);
+            acc[i][4 * j + 3] = __fmaf_rn(av, b4[j].w, acc[i][4 * j + 3]);
+          }
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+
+  // Epilogue: direct stores (split-K slices go to the partial buffer).
+  float* C;
+  long ldc;
+  if (p.splits > 1) {
+    C = p.partial + ((long)batch * p.splits + split) * (long)p.M * p.N;
+    ldc = p.N;
+  } else {
+    C = p.C + batch * p.strideC;
+    ldc = p.ldc;
+  }
+  const bool vec_store = p.splits > 1 ? ((p.N & 3) == 0) : p.vec_store;
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int r = m0 + wm * WM + tm + 8 * i;
+    if (r >= p.M) continue;
+    float* crow = C + (long)r * ldc;
+#pragma unroll
+    for (int j = 0; j < TN / 4; ++j) {
+      const int c = n0 + wn * WN + 16 * j + 4 * tn;
+      if (vec_store && c + 3 < p.N) {
+        *reinterpret_cast<float4*>(crow + c) =
+            make_float4(acc[i][4 * j], acc[i][4 * j + 1], acc[i][4 * j + 2], acc[i][4 * j + 3]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (c + e < p.N) crow[c + e] = acc[i][4 * j + e];
+      }
+    }
+  }
+}
+
+// Fixed-order reduction of split-K partial slices: C = ((p0 + p1) + p2) + ...
+__global__ void splitk_reduce_kernel(const float* __restrict__ partial, float* __restrict__ C,
+                                     int M, int N, long ldc, long strideC, int splits, int batches) {
+  const long MN = (long)M * N;
+  const long total = MN * batches;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const long b = idx / MN;
+    const long e = idx - b * MN;
+    const float* src = partial + b * splits * MN + e;
+    float s = src[0];
+    for (int k = 1; k < splits; ++k) s += src[k * MN];
+    const long r = e / N;
+    const long c = e - r * N;
+    C[b * strideC + r * ldc + c] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tile table and launcher.
+
+struct FfmaEntry {
+  int bm, bn, bk, wm, wn, stages;
+  int threads, smem;
+  cudaError_t (*launch)(const FfmaParams&, dim3, cudaStream_t, bool vec);
+};
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+static cudaError_t launch_ffma(const FfmaParams& p, dim3 grid, cudaStream_t st, bool vec) {
+  using S = FfmaShape<BM, BN, BK, WM, WN, STAGES>;
+  auto kv = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, true>;
+  auto ks = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false>;
+  auto k = vec ? kv : ks;
+  static uint32_t mask_v = 0, mask_s = 0;
+  if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, vec ? &mask_v : &mask_s))
+    return cudaErrorInvalidValue;
+  k<<<grid, S::kThreads, S::kSmemBytes, st>>>(p);
+  return cudaGetLastError();
+}
+
+#define HBSG_FFMA_ENTRY(BM, BN, BK, WM, WN, ST)                                           \
+  FfmaEntry {                                                                             \
+    BM, BN, BK, WM, WN, ST, FfmaShape<BM, BN, BK, WM, WN, ST>::kThreads,                  \
+        FfmaShape<BM, BN, BK, WM, WN, ST>::kSmemBytes, &launch_ffma<BM, BN, BK, WM, WN, ST> \
+  }
+
+static const FfmaEntry kFfmaTiles[] = {
+    HBSG_FFMA_ENTRY(128, 256, 16, 64, 64, 4),  // 1: 8 warps, 128 FMA per thread per k
+    HBSG_FFMA_ENTRY(128, 128, 16, 64, 64, 4),  // 2: 4 warps
+    HBSG_FFMA_ENTRY(64, 64, 16, 32, 32, 4),    // 3: 4 warps, small problems
+    HBSG_FFMA_ENTRY(128, 64, 16, 64, 32, 4),   // 4: 4 warps, narrow N
+    HBSG_FFMA_ENTRY(128, 256, 32, 64, 64, 3),  // 5: 8 warps, deeper K tile
+    HBSG_FFMA_ENTRY(256, 128, 16, 64, 64, 4),  // 6: 8 warps, tall
+};
+static constexpr int kNumFfmaTiles = sizeof(kFfmaTiles) / sizeof(kFfmaTiles[0]);
+
+int ffma_num_tiles() { return kNumFfmaTiles; }
+
+bool ffma_tile_info(int idx, hbsg_tile_info* out) {
+  if (idx < 0 || idx >= kNumFfmaTiles) return false;
+  const FfmaEntry& e = kFfmaTiles[idx];
+  out->variant_class = 0;
+  out->bm = e.bm;
+  out->bn = e.bn;
+  out->bk = e.bk;
+  out->threads = e.threads;
+  out->smem_bytes = e.smem;
+  return true;
+}
+
+// Pick the tile with the best estimated SM utilisation, preferring the large
+// tile when the wave count is high (fewer bytes per flop).
+int ffma_pick_tile(int M, int N, int K, int batch, int num_sms) {
+  (void)K;
+  double best = -1.0;
+  int best_idx = 0;
+  const int cand[] = {0, 1, 3, 2};
+  for (int idx : cand) {
+    const FfmaEntry& e = kFfmaTiles[idx];
+    const long tiles = (long)((M + e.bm - 1) / e.bm) * ((N + e.bn - 1) / e.bn) * batch;
+    const int per_sm = e.threads <= 128 ? 2 : 1;
+    const double slots = (double)num_sms * per_sm;
+    const double waves = tiles / slots;
+    const double eff = waves / ceil(waves);  // tail efficiency
+    // work per tile relative to the biggest tile: bigger tiles amortise loads
+    const double tile_eff = (e.bm * e.bn >= 128 * 256) ? 1.0 : (e.bm * e.bn >= 128 * 128 ? 0.93 : 0.8);
+    const double fill = fmin(1.0, tiles / slots);
+    const double score = eff * tile_eff * (fill < 1.0 ? fill : 1.0);
+    if (score > best + 1e-9) {
+      best = score;
+      best_idx = idx;
+    }
+  }
+  return best_idx;
+}
+
+size_t ffma_workspace_bytes(int M, int N, int batch, int splits) {
+  return splits > 1 ? (size_t)M * N * batch * splits * sizeof(float) : 0;
+}
+
+cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st) {
+  const FfmaEntry& e = kFfmaTiles[tile_idx];
+  p.tiles_m = (p.M + e.bm - 1) / e.bm;
+  p.tiles_n = (p.N + e.bn - 1) / e.bn;
+  if (p.raster <= 0) p.raster = 8;
+  if (p.splits < 1) p.splits = 1;
+  if (p.splits > 1) {
+    // K slices are whole BK tiles.
+    int per = (p.K + p.splits - 1) / p.splits;
+    per = (per + e.bk - 1) / e.bk * e.bk;
+    p.k_per_split = per;
+    p.splits = (p.K + per - 1) / per;
+  } else {
+    p.k_per_split = p.K;
+  }
+  const bool vec = ((p.lda & 3) == 0) && ((p.ldb & 3) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(p.A) & 15) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(p.B) & 15) == 0) && ((p.strideA & 3) == 0) &&
+                   ((p.strideB & 3) == 0);
+  p.vec_store = ((p.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
+                ((p.strideC & 3) == 0);
+  dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)p.splits, (unsigned)batch);
+  cudaError_t err = e.launch(p, grid, st, vec);
+  if (err != cudaSuccess || p.splits == 1) return err;
+  const long total = (long)p.M * p.N * batch;
+  long nb = (total + 255) / 256;
+  int blocks = (int)(nb < 148L * 16 ? nb : 148L * 16);
+  splitk_reduce_kernel<<<blocks, 256, 0, st>>>(p.partial, p.C, p.M, p.N, p.ldc, p.strideC,
+                                               p.splits, batch);
+  return cudaGetLastError();
+}
+
+}  // namespace hbsg

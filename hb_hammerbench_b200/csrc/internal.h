@@ -1,0 +1,42 @@
+// Internal interfaces between the C-ABI layer (api.cu) and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/hbsg.h"
+
+namespace hbsg {
+
+// ---- FFMA family ------------------------------------------------------------
+struct FfmaParams {
+  const float* A;
+  const float* B;
+  float* C;
+  float* partial;  // split-K slices, [batch][split][M][N]
+  long lda, ldb, ldc;
+  long strideA, strideB, strideC;  // batch strides in elements
+  int M, N, K;
+  int k_per_split;
+  int splits;
+  int tiles_m, tiles_n;
+  int raster;
+  bool vec_store;
+};
+
+int ffma_num_tiles();
+bool ffma_tile_info(int idx, hbsg_tile_info* out);
+int ffma_pick_tile(int M, int N, int K, int batch, int num_sms);
+size_t ffma_workspace_bytes(int M, int N, int batch, int splits);
+cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st);
+
+// ---- device state -------------------------------------------------------------
+// Returns the SM count of the current device (cached per device), or -1 when
+// no sm_100 device is current.
+int current_device_sms(int* device_out);
+
+// Sets a kernel's dynamic shared memory limit once per device.
+bool set_smem_once(const void* func, int bytes, uint32_t* device_mask);
+
+}  // namespace hbsg

@@ -1,0 +1,142 @@
+"""Host-side interface of the SGEMM hot path (torch tensors in, C ABI under).
+
+Mirrors the HammerBench sgemm benchmark's host flow (apps/sgemm/main.cpp):
+  sgemm(mat1, mat2, result, n, niter)  ~ the enqueue of `kernel` with argv
+                                         {mat1, mat2, result, pod}
+                                         (main.cpp:86-98): NITER independent
+                                         n x n row-major products, matrix i at
+                                         element offset n*n*i.
+  gemm(a, b, c, ...)                   ~ the legacy rectangular kernel_mm_opt
+                                         (apps/legacy/gemm/sgemm_data_parallel/
+                                         kernel.cpp:323-344) with strides.
+Every call goes through libhbsg.so on the tensors' device and the current
+torch stream; errors raise HbsgError with the library's status.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import Config, HbsgError, TileInfo, check, lib  # noqa: F401
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _variant(v) -> int:
+    if isinstance(v, str):
+        return _lib.VARIANTS[v.lower()]
+    return int(v)
+
+
+def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p:
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _check_f32_cuda(name: str, t: torch.Tensor) -> None:
+    if t.dtype != torch.float32 or not t.is_cuda:
+        raise TypeError(f"{name} must be a float32 CUDA tensor")
+
+
+def _config(cfg) -> ctypes.POINTER(Config) | None:
+    if cfg is None:
+        return None
+    if isinstance(cfg, dict):
+        cfg = Config(**cfg)
+    return ctypes.pointer(cfg)
+
+
+def sgemm_workspace_size(n: int, niter: int, variant="ffma") -> int:
+    return int(lib().hbsg_sgemm_workspace_size(n, niter, _variant(variant)))
+
+
+def gemm_workspace_size(m: int, n: int, k: int, variant="ffma", config=None) -> int:
+    return int(lib().hbsg_gemm_workspace_size(m, n, k, _variant(variant), _config(config)))
+
+
+def _workspace(nbytes: int, device, workspace: torch.Tensor | None):
+    if nbytes == 0:
+        return workspace
+    if workspace is not None and workspace.numel() * workspace.element_size() >= nbytes:
+        return workspace
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def sgemm(mat1: torch.Tensor, mat2: torch.Tensor, result: torch.Tensor | None = None,
+          n: int | None = None, niter: int | None = None, variant="ffma",
+          workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """result[i] = mat1[i] @ mat2[i] for i < niter (each n x n, contiguous)."""
+    _check_f32_cuda("mat1", mat1)
+    _check_f32_cuda("mat2", mat2)
+    if not (mat1.is_contiguous() and mat2.is_contiguous()):
+        raise ValueError("mat1 and mat2 must be contiguous")
+    if n is None:
+        n = mat1.shape[-1]
+    if niter is None:
+        niter = mat1.numel() // (n * n) if n else 0
+    if mat1.numel() < niter * n * n or mat2.numel() < niter * n * n:
+        raise ValueError("buffers smaller than niter*n*n")
+    if result is None:
+        result = torch.empty_like(mat1)
+    _check_f32_cuda("result", result)
+    v = _variant(variant)
+    with torch.cuda.device(mat1.device):
+        if v == _lib.FFMA and workspace is None:
+            st = lib().hbsg_sgemm(_ptr(mat1), _ptr(mat2), _ptr(result), n, niter, _stream())
+            check(st, "hbsg_sgemm")
+        else:
+            need = sgemm_workspace_size(n, niter, v)
+            ws = _workspace(need, mat1.device, workspace)
+            st = lib().hbsg_sgemm_variant(_ptr(mat1), _ptr(mat2), _ptr(result), n, niter, v,
+                                          _ptr(ws), need, _stream())
+            check(st, "hbsg_sgemm_variant")
+    return result
+
+
+def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, variant="ffma",
+         trans_a: bool = False, trans_b: bool = False, config=None,
+         workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """c = op(a) @ op(b) for 2-D float32 CUDA tensors with unit inner stride.
+    With trans_a, `a` holds A^T (k x m); with trans_b, `b` holds B^T (n x k)."""
+    _check_f32_cuda("a", a)
+    _check_f32_cuda("b", b)
+    if a.dim() != 2 or b.dim() != 2 or a.stride(1) != 1 or b.stride(1) != 1:
+        raise ValueError("a and b must be 2-D with unit inner stride")
+    m, k = (a.shape[1], a.shape[0]) if trans_a else (a.shape[0], a.shape[1])
+    kb, n = (b.shape[1], b.shape[0]) if trans_b else (b.shape[0], b.shape[1])
+    if k != kb:
+        raise ValueError(f"inner dimensions differ: {k} vs {kb}")
+    if c is None:
+        c = torch.empty((m, n), dtype=torch.float32, device=a.device)
+    _check_f32_cuda("c", c)
+    if c.dim() != 2 or c.stride(1) != 1 or tuple(c.shape) != (m, n):
+        raise ValueError("c must be m x n with unit inner stride")
+    v = _variant(variant)
+    cfgp = _config(config)
+    with torch.cuda.device(a.device):
+        need = int(lib().hbsg_gemm_workspace_size(m, n, k, v, cfgp))
+        ws = _workspace(need, a.device, workspace)
+        st = lib().hbsg_gemm_ex(int(trans_a), int(trans_b), m, n, k, _ptr(a), a.stride(0),
+                                _ptr(b), b.stride(0), _ptr(c), c.stride(0), v, cfgp,
+                                _ptr(ws), need, _stream())
+        check(st, "hbsg_gemm_ex")
+    return c
+
+
+def tiles() -> list[dict]:
+    """The tile-shape table (1-based ids) the autotuner searches."""
+    out = []
+    for t in range(1, lib().hbsg_num_tiles() + 1):
+        info = TileInfo()
+        check(lib().hbsg_tile_describe(t, ctypes.byref(info)), "hbsg_tile_describe")
+        out.append({"tile": t, "family": "ffma" if info.variant_class == 0 else "bf16",
+                    "bm": info.bm, "bn": info.bn, "bk": info.bk,
+                    "threads": info.threads, "smem_bytes": info.smem_bytes})
+    return out
+
+
+def check_device() -> None:
+    check(lib().hbsg_check_device(_stream()), "device check")

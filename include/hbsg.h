@@ -1,0 +1,134 @@
+/*
+ * hbsg.h -- C ABI of the B200 (sm_100a) SGEMM hot path that stands in for the
+ * HammerBench `apps/sgemm` benchmark kernel.
+ *
+ * Conventions
+ *   - All matrices are FP32, row-major unless a trans flag says otherwise,
+ *     in caller-owned device memory. The library allocates nothing: every
+ *     scratch buffer is caller-provided (`workspace`, sized by the matching
+ *     *_workspace_size query).
+ *   - Every entry point is asynchronous on `stream` (a cudaStream_t; NULL is
+ *     the legacy default stream) and returns an hbsg_status (0 = success,
+ *     negative = error). Argument errors are detected before anything is
+ *     launched and never abort the process.
+ *   - Thread-safe for calls on distinct streams with distinct workspaces.
+ */
+#ifndef HBSG_H
+#define HBSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same object as cudaStream_t; declared here so callers need no CUDA header. */
+typedef struct CUstream_st* hbsg_stream_t;
+
+typedef enum hbsg_status {
+    HBSG_OK = 0,
+    HBSG_ERR_INVALID_ARG = -1,    /* null pointer, bad size, bad leading dim */
+    HBSG_ERR_UNSUPPORTED = -2,    /* variant/config/alignment not supported */
+    HBSG_ERR_WORKSPACE = -3,      /* workspace missing, misaligned or too small */
+    HBSG_ERR_LAUNCH = -4,         /* kernel launch failed */
+    HBSG_ERR_DEVICE_TIMEOUT = -5, /* a bounded device-side wait expired */
+    HBSG_ERR_NO_DEVICE = -6,      /* no sm_100 device current */
+    HBSG_ERR_CUDA = -7            /* other CUDA runtime error */
+} hbsg_status;
+
+/* Arithmetic forms of C = A*B. */
+typedef enum hbsg_variant {
+    HBSG_FFMA = 0,          /* FP32 SIMT: one fused multiply-add per k, k ascending */
+    HBSG_BF16X3 = 1,        /* split-BF16 (hi, mid), 3 tensor-core products */
+    HBSG_BF16X6 = 2,        /* split-BF16 (hi, mid, lo), 6 tensor-core products */
+    HBSG_BF16X3_SCALED = 3, /* as BF16X3 after exact per-row (A) / per-column (B) 2^e scaling */
+    HBSG_BF16X6_SCALED = 4  /* as BF16X6 after exact per-row (A) / per-column (B) 2^e scaling */
+} hbsg_variant;
+
+/* Explicit schedule (used by the autotuner). Fields left at 0 mean "library
+ * heuristic". */
+typedef struct hbsg_config {
+    int tile;          /* tile-shape id, 1-based index into hbsg_tile_info (0 = heuristic) */
+    int split_k;       /* number of K slices (0/1 = none); slices are reduced in fixed order */
+    int raster_group;  /* tile rows per rasterisation group (0 = heuristic) */
+    int chunk_k;       /* split-BF16: K elements accumulated on the tensor core before the
+                          partial is added in FP32 registers (0 = heuristic) */
+} hbsg_config;
+
+typedef struct hbsg_tile_info {
+    int variant_class; /* 0 = FFMA kernel family, 1 = split-BF16 tensor-core family */
+    int bm, bn, bk;    /* CTA tile */
+    int threads;       /* threads per CTA */
+    int smem_bytes;    /* dynamic shared memory per CTA */
+} hbsg_tile_info;
+
+/* ---------------------------------------------------------------------------
+ * Benchmark entry point.
+ *
+ * Replaces the device kernel `int kernel(float* mat1, float* mat2,
+ * float* result, int pod_id)` (apps/sgemm/kernel.cpp:279-333) together with
+ * its launch `hb_mc_kernel_enqueue(..., "kernel", 4, {mat1, mat2, result,
+ * pod})` + `hb_mc_device_pods_kernels_execute` (apps/sgemm/main.cpp:86-98).
+ * N and NITER were compile-time macros there (apps/sgemm/template.mk:30-31);
+ * here they are arguments. result[i] = mat1[i] * mat2[i] for i < niter, each
+ * an n x n row-major matrix at element offset n*n*i (kernel.cpp:293-297).
+ * Arithmetic is that of the reference device kernel: every output starts at
+ * 0.0f and receives one fused multiply-add per k in ascending k
+ * (kernel.cpp:24-32,208-263), so results are bit-identical to it.
+ */
+int hbsg_sgemm(const float* mat1, const float* mat2, float* result,
+               int n, int niter, hbsg_stream_t stream);
+
+/* Same batch layout with a chosen variant (split-BF16 needs a workspace). */
+int hbsg_sgemm_variant(const float* mat1, const float* mat2, float* result,
+                       int n, int niter, int variant,
+                       void* workspace, size_t workspace_bytes,
+                       hbsg_stream_t stream);
+size_t hbsg_sgemm_workspace_size(int n, int niter, int variant);
+
+/* ---------------------------------------------------------------------------
+ * General strided GEMM C[m x n] = op(A)[m x k] * op(B)[k x n].
+ *
+ * Follows the rectangular interface of the legacy data-parallel kernel
+ * `kernel_mm_opt(hb_tensor_t* result, hb_tensor_t* mat1, hb_tensor_t* mat2)`
+ * (apps/legacy/gemm/sgemm_data_parallel/kernel.cpp:323-344, sizes and
+ * strides from hb_tensor.hpp:26-54), with optional transposed operands
+ * (its transposed-A load, kernel.cpp:21-48). trans_a != 0 means A is stored
+ * k x m (element (i,p) at a[p*lda + i]); likewise trans_b (B stored n x k).
+ */
+int hbsg_gemm(int trans_a, int trans_b, int m, int n, int k,
+              const float* a, int64_t lda, const float* b, int64_t ldb,
+              float* c, int64_t ldc, int variant,
+              void* workspace, size_t workspace_bytes, hbsg_stream_t stream);
+
+/* As hbsg_gemm with an explicit schedule (cfg may be NULL). */
+int hbsg_gemm_ex(int trans_a, int trans_b, int m, int n, int k,
+                 const float* a, int64_t lda, const float* b, int64_t ldb,
+                 float* c, int64_t ldc, int variant, const hbsg_config* cfg,
+                 void* workspace, size_t workspace_bytes, hbsg_stream_t stream);
+
+size_t hbsg_gemm_workspace_size(int m, int n, int k, int variant,
+                                const hbsg_config* cfg);
+
+/* Tile-shape table for the autotuner: number of ids and their description. */
+int hbsg_num_tiles(void);
+int hbsg_tile_describe(int tile, hbsg_tile_info* out);
+
+/* ---------------------------------------------------------------------------
+ * Error reporting.
+ */
+const char* hbsg_strerror(int status);
+
+/* Synchronises `stream`, then reports and clears the device-side error flag
+ * raised by bounded waits inside the kernels (HBSG_OK if none). */
+int hbsg_check_device(hbsg_stream_t stream);
+
+/* ABI version (major * 100 + minor). */
+int hbsg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HBSG_H */

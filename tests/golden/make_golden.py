@@ -1,0 +1,86 @@
+"""Generate the golden fixtures under tests/golden/ from the reference's own
+host reference product, host_mm (apps/sgemm/main.cpp:15-26), compiled from the
+reference source tree by `make -C oracle ref`.
+
+Run in a container that has the reference tree:  python tests/golden/make_golden.py
+The fixtures are committed; the tests never need the reference tree.
+
+Fixtures
+  sgemm_mod_N512_NITER2.json    the benchmark's own launch N_512__NITER_2 with its
+                                inputs mat1[i] = i % 7, mat2[i] = i % 3
+                                (main.cpp:49-52, tests.mk:1): SHA-256 of the
+                                expected float32 result bytes and sampled values.
+  sgemm_ramp_identity_N512.json legacy sgemm_512 fixture, A[i] = i, B = I, C = A
+                                (apps/legacy/gemm/sgemm_512/main.cpp:69-80).
+  sgemm_uniform_N64_NITER2.npz  seeded U[-1,1) inputs (numpy PCG64, seed 42) and
+  sgemm_uniform_N128_NITER1.npz the reference host_mm outputs, per matrix.
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle  # noqa: E402
+
+
+def sha(x: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(x, np.float32).tobytes()).hexdigest()
+
+
+def main():
+    oracle.build()
+    assert oracle.ref_available(), "reference host_mm not built"
+
+    # 1. the benchmark's own fixture, N=512 NITER=2
+    n, niter = 512, 2
+    m1, m2 = oracle.fill_mod(niter * n * n)
+    outs = {}
+    for opt in ("O3", "O0"):
+        outs[opt] = np.concatenate([
+            oracle.ref_host_mm(m1[i * n * n:(i + 1) * n * n], m2[i * n * n:(i + 1) * n * n], n, opt).ravel()
+            for i in range(niter)])
+    assert np.array_equal(outs["O3"], outs["O0"])
+    c = outs["O3"]
+    rng = np.random.Generator(np.random.PCG64(7))
+    idx = np.sort(rng.choice(c.size, 64, replace=False))
+    fix = {
+        "source": "reference host_mm (apps/sgemm/main.cpp:15-26) compiled from the reference tree, -O3 and -O0 agree",
+        "inputs": "mat1[i] = i % 7, mat2[i] = i % 3 for i < NITER*N*N (apps/sgemm/main.cpp:49-52)",
+        "N": n, "NITER": niter,
+        "sha256_result_f32": sha(c),
+        "first": float(c[0]), "last": float(c[-1]),
+        "sum_per_matrix": [float(np.sum(c[i * n * n:(i + 1) * n * n].astype(np.float64))) for i in range(niter)],
+        "samples": [[int(i), float(c[i])] for i in idx],
+    }
+    with open(os.path.join(HERE, "sgemm_mod_N512_NITER2.json"), "w") as f:
+        json.dump(fix, f, indent=1)
+
+    # 2. legacy sgemm_512 fixture: C = A
+    a, b = oracle.fill_ramp_identity(n)
+    cr = oracle.ref_host_mm(a, b, n, "O3")
+    assert np.array_equal(cr, a)
+    with open(os.path.join(HERE, "sgemm_ramp_identity_N512.json"), "w") as f:
+        json.dump({
+            "source": "reference host_mm compiled from the reference tree",
+            "inputs": "A[i] = i, B = identity (apps/legacy/gemm/sgemm_512/main.cpp:69-80)",
+            "N": n, "sha256_result_f32": sha(cr), "result_equals_A": True,
+        }, f, indent=1)
+
+    # 3. seeded uniform inputs with the reference's outputs
+    for n, niter in ((64, 2), (128, 1)):
+        A, B = oracle.uniform_inputs((niter, n, n), (niter, n, n), seed=42)
+        C = np.stack([oracle.ref_host_mm(A[i], B[i], n, "O3") for i in range(niter)])
+        C0 = np.stack([oracle.ref_host_mm(A[i], B[i], n, "O0") for i in range(niter)])
+        assert np.array_equal(C, C0)
+        np.savez_compressed(os.path.join(HERE, f"sgemm_uniform_N{n}_NITER{niter}.npz"),
+                            A=A, B=B, C_ref=C, seed=np.int64(42))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
