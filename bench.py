@@ -2,27 +2,33 @@
 """Benchmark of the SGEMM hot path: C = A*B in FP32 at M = N = K = 8192.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--variant ffma|bf16x3|bf16x6|...] [--n 8192]
+                    [--variant bf16x6|bf16x3|bf16x6_scaled|bf16x3_scaled|ffma] [--n 8192]
 
-One step = one C-ABI call computing C = A*B for one 8192^3 problem (the
-square sweep's largest size). Inputs are seeded i.i.d. U[-1,1) float32 built
-on the device; each operand is 268 MB, larger than the 126 MB L2, so no flush
-is needed between steps. `value` is effective FP32 TFLOP/s = 2*N^3 / step
-time, summed over ranks (every rank runs its own replica; the path does not
-shard). The error of the last step's C against an FP64 product is stated in
-the line. `e2e` repeats the measurement through the public API with pinned
-host buffers, the H2D copies of A and B and the D2H copy of C inside the
-timed region.
+Metric: effective FP32 TFLOP/s (2*N^3 / step time) at a stated error against
+an FP64 product. One step = one full C = A*B through the C ABI: for the
+split-BF16 forms the split pass (split-only call) followed by the
+tensor-core product (pre-split call), for FFMA one call. Inputs are seeded
+i.i.d. U[-1,1) float32 built on the device; each operand is 268 MB (larger
+than the 126 MB L2), so no flush is needed between steps. `value` sums over
+ranks: every rank runs its own replica (the path does not shard).
+
+The same line carries the plain FFMA kernel on the same inputs ("ffma"), the
+error of both against the FP64 product, `e2e` (the public call with pinned
+host buffers: H2D of A and B and D2H of C inside the timed region), the
+roofline of the dominant kernel, the clocks seen during the timed region and
+the CPU baseline (the reference host_mm loop on the host cores).
 
 --impl reference times the reference's CPU implementation of the path (the
-host_mm loop, restated in oracle/oracle.c) on the host cores, on a row sample
-of the same workload (rows are independent, so cost is linear in rows).
+host_mm loop of apps/sgemm/main.cpp:15-26, restated in oracle/oracle.c) on
+the host cores, on a row sample of the same workload (rows are independent,
+so cost is linear in rows).
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -32,8 +38,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+METRIC = "effective FP32 TFLOP/s at stated error vs FP64: split-BF16 TC vs plain FFMA, 1 B200"
 SMS = 148
 FP32_LANES_PER_SM = 128
+PRODUCTS = {"bf16x3": 3, "bf16x6": 6, "bf16x3_scaled": 3, "bf16x6_scaled": 6}
 
 
 def _peaks():
@@ -44,6 +52,16 @@ def _peaks():
         return d
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
             "sm_max_mhz": 1965.0, "source": "fallback"}
+
+
+def _profile_traffic(name: str):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/<name>.md
+    (line `dram_bytes_per_launch: <int>`), or None."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9]+)", open(p).read())
+    return int(m.group(1)) if m else None
 
 
 # ---------------------------------------------------------------------------
@@ -79,7 +97,7 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], [], set()
+        sm, mx, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
@@ -88,6 +106,7 @@ class ClockSampler:
             try:
                 sm.append(float(f[1]))
                 mx.append(float(f[2]))
+                pw.append(float(f[3]))
             except ValueError:
                 continue
             for name, val in zip(names, f[5:9]):
@@ -96,6 +115,7 @@ class ClockSampler:
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -109,13 +129,11 @@ def cpu_baseline(n: int, seconds: float = 12.0, threads: int = 0) -> dict:
     rng = np.random.Generator(np.random.PCG64(42))
     B = rng.uniform(-1, 1, size=(n, n)).astype(np.float32)
     nthreads = threads or len(os.sched_getaffinity(0))
-    # probe the rate with one row per thread, then size the sample
     rows = nthreads
-    A = rng.uniform(-1, 1, size=(max(rows, 1), n)).astype(np.float32)
+    A = rng.uniform(-1, 1, size=(rows, n)).astype(np.float32)
     t0 = time.perf_counter()
-    oracle.host_mm(A[:rows], B, threads=nthreads)
-    dt = time.perf_counter() - t0
-    per_row = dt / rows
+    oracle.host_mm(A, B, threads=nthreads)
+    per_row = (time.perf_counter() - t0) / rows
     rows = int(max(nthreads, min(n, seconds / max(per_row, 1e-9))))
     rows = max(nthreads, rows // nthreads * nthreads)
     A = rng.uniform(-1, 1, size=(rows, n)).astype(np.float32)
@@ -143,7 +161,6 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     n = args.n
-    # each step is a bounded row sample; W + K steps fit in about a minute
     per_step = max(2.0, 60.0 / (args.steps + args.warmup))
     vals = []
     cb = None
@@ -154,12 +171,11 @@ def run_reference(args) -> None:
     v = statistics.median(vals)
     flops = 2.0 * n ** 3
     line = {
-        "impl": "reference",
-        "metric": "effective FP32 TFLOP/s at stated error vs FP64: split-BF16 TC vs plain FFMA, 1 B200",
+        "impl": "reference", "metric": METRIC,
         "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": flops / (v * 1e12) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic U[-1,1) seeded",
+        "data": "synthetic: seeded i.i.d. U[-1,1) float32",
         "config": {"workload": f"sgemm M=N=K={n} fp32 row-major", "m": n, "n": n, "k": n},
         "cpu_baseline": {**cb, "value": v},
         "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -167,71 +183,119 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _err(C, ref) -> dict:
+    import torch
+    d = C.double() - ref
+    return {"max_abs": float(d.abs().max()),
+            "rel_fro": float(torch.linalg.norm(d) / torch.linalg.norm(ref))}
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
 
     import hb_hammerbench_b200 as hb
+    from hb_hammerbench_b200 import _lib
 
     ws, rank, local = _dist()
     if ws > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.n
     variant = args.variant
+    split = variant != "ffma"
+    flops = 2.0 * n ** 3
+    warmup = max(3, args.warmup)
+
     g = torch.Generator(device=dev).manual_seed(42 + rank)
     A = torch.rand((n, n), device=dev, generator=g) * 2 - 1
     B = torch.rand((n, n), device=dev, generator=g) * 2 - 1
     C = torch.empty((n, n), device=dev)
     wsz = hb.gemm_workspace_size(n, n, n, variant)
-    wsp = torch.empty(max(wsz, 1), dtype=torch.uint8, device=dev)
+    wsp = torch.empty(max(wsz, 256), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
-
-    def step():
-        hb.gemm(A, B, C, variant=variant, workspace=wsp)
+    split_only = {"flags": _lib.FLAG_SPLIT_ONLY}
+    presplit = {"flags": _lib.FLAG_PRESPLIT_A | _lib.FLAG_PRESPLIT_B}
 
     def barrier():
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(max(3, args.warmup)):
-        step()
-    barrier()
+    def timed(step_fn, steps, per_step=True):
+        """K steps on `stream`; returns (total ms max over ranks, per-step kernel ms)."""
+        for _ in range(warmup):
+            step_fn(None)
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        t0.record(stream)
+        for i in range(steps):
+            step_fn(evs[i] if per_step else None)
+        t1.record(stream)
+        barrier()
+        total = torch.tensor([t0.elapsed_time(t1)], device=dev)
+        if ws > 1:
+            dist.all_reduce(total, op=dist.ReduceOp.MAX)
+        return float(total.item()), ([a.elapsed_time(b) for a, b in evs] if per_step else [])
+
+    def step_main(ev):
+        if split:
+            hb.gemm(A, B, C, variant=variant, workspace=wsp, config=split_only)
+            if ev:
+                ev[0].record(stream)
+            hb.gemm(A, B, C, variant=variant, workspace=wsp, config=presplit)
+            if ev:
+                ev[1].record(stream)
+        else:
+            if ev:
+                ev[0].record(stream)
+            hb.gemm(A, B, C, variant="ffma")
+            if ev:
+                ev[1].record(stream)
+
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    barrier()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    for i in range(args.steps):
-        evs[i][0].record(stream)
-        step()
-        evs[i][1].record(stream)
-    t_end.record(stream)
-    barrier()
+    total_ms, kern_ms = timed(step_main, args.steps)
     clocks = sampler.stop()
-    total_ms = t_start.elapsed_time(t_end)
-    launch_ms = [a.elapsed_time(b) for a, b in evs]
-    t = torch.tensor([total_ms], device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    flops = 2.0 * n ** 3
     value = ws * flops * args.steps / (total_ms * 1e-3) / 1e12
 
-    # error of the last result against an FP64 product (outside the timed region)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "variant": variant, "ms_per_step": ms_per_step}),
+                  flush=True)
+        if ws > 1:
+            dist.destroy_process_group()
+        return
+
     ref = A.double() @ B.double()
-    d = C.double() - ref
-    err = {"max_abs": float(d.abs().max()),
-           "rel_fro": float(torch.linalg.norm(d) / torch.linalg.norm(ref)),
-           "reference": "FP64 product of the same inputs (torch float64 matmul on the GPU)"}
-    del ref, d
+    err = _err(C, ref)
+
+    # plain FFMA kernel on the same inputs, for the comparison the metric names
+    ffma = None
+    if split and not args.no_compare:
+        C2 = torch.empty_like(C)
+
+        def step_ffma(ev):
+            if ev:
+                ev[0].record(stream)
+            hb.gemm(A, B, C2, variant="ffma")
+            if ev:
+                ev[1].record(stream)
+        f_total, f_kern = timed(step_ffma, max(3, args.steps // 2))
+        f_steps = max(3, args.steps // 2)
+        f_val = ws * flops * f_steps / (f_total * 1e-3) / 1e12
+        ffma = {"value": f_val, "unit": "TFLOP/s", "ms_per_step": f_total / f_steps,
+                "error_vs_fp64": _err(C2, ref), "kernel": "ffma_sgemm_kernel (tile 1: 128x128, packed FMA)"}
+        del C2
+    del ref
 
     # e2e through the public API with pinned host buffers
     hA = A.cpu().pin_memory()
@@ -240,60 +304,65 @@ def run_ours(args) -> None:
     dA = torch.empty_like(A)
     dB = torch.empty_like(B)
 
-    def e2e_step():
+    def step_e2e(ev):
         dA.copy_(hA, non_blocking=True)
         dB.copy_(hB, non_blocking=True)
         hb.gemm(dA, dB, C, variant=variant, workspace=wsp)
         hC.copy_(C, non_blocking=True)
-
-    for _ in range(2):
-        e2e_step()
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    te = torch.tensor([e2e_ms], device=dev)
-    if ws > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te.item())
-    e2e_val = ws * flops * args.steps / (e2e_ms * 1e-3) / 1e12
+    e_total, _ = timed(step_e2e, args.steps, per_step=False)
+    e2e_val = ws * flops * args.steps / (e_total * 1e-3) / 1e12
     assert torch.equal(hC, C.cpu())
 
     peaks = _peaks()
-    avg_launch = statistics.mean(launch_ms)
-    achieved = flops / (avg_launch * 1e-3) / 1e12
-    sm_max = clocks.get("sm_max_mhz") or peaks["sm_max_mhz"]
-    peak_fp32 = SMS * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
-    roof = {"bound": "fp32_simt", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
-            "frac": achieved / peak_fp32, "traffic": None,
-            "kernel": "ffma_sgemm_kernel", "algorithmic_flops_per_launch": flops,
-            "peak_note": f"derived: {SMS} SM x {FP32_LANES_PER_SM} FP32 lanes x 2 x {sm_max:.0f} MHz "
-                         "(no measured FP32 peak exists)"}
-    if clocks.get("sm_mhz"):
-        roof["frac_at_measured_clock"] = achieved / (peak_fp32 * clocks["sm_mhz"] / sm_max)
+    avg_kernel_ms = statistics.mean(kern_ms)
+    if split:
+        prods = PRODUCTS[variant]
+        mma_flops = prods * flops
+        achieved = mma_flops / (avg_kernel_ms * 1e-3) / 1e12
+        traffic = _profile_traffic(f"tc_gemm_{variant}_n{n}")
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
+                "kernel": "tc_gemm_kernel", "algorithmic_flops_per_launch": mma_flops,
+                "flops_note": f"{prods} BF16 products x 2*N^3 executed on the tensor cores per launch; "
+                              f"peak = {peaks['source']} cuBLAS bf16 burst",
+                "frac_of_sustained": achieved / peaks["bf16_tflops_sustained"],
+                "kernel_ms": avg_kernel_ms,
+                "effective_fp32_tflops_of_kernel": flops / (avg_kernel_ms * 1e-3) / 1e12}
+        launches = args.steps * (3 + (2 if "scaled" in variant else 0))
+    else:
+        achieved = flops / (avg_kernel_ms * 1e-3) / 1e12
+        sm_max = clocks.get("sm_max_mhz") or peaks["sm_max_mhz"]
+        peak_fp32 = SMS * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
+        roof = {"bound": "fp32_simt", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                "frac": achieved / peak_fp32, "traffic": _profile_traffic(f"ffma_sgemm_n{n}"),
+                "kernel": "ffma_sgemm_kernel", "algorithmic_flops_per_launch": flops,
+                "flops_note": f"derived peak: {SMS} SM x {FP32_LANES_PER_SM} FP32 lanes x 2 x "
+                              f"{sm_max:.0f} MHz (no measured FP32 peak exists)",
+                "kernel_ms": avg_kernel_ms}
+        launches = args.steps
 
     line = {
-        "metric": "effective FP32 TFLOP/s at stated error vs FP64: split-BF16 TC vs plain FFMA, 1 B200",
+        "metric": METRIC,
         "value": value, "unit": "TFLOP/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "warmup": warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded i.i.d. U[-1,1) float32, built on the device",
         "config": {"workload": f"sgemm M=N=K={n} fp32 row-major, variant {variant}",
                    "m": n, "n": n, "k": n, "variant": variant,
-                   "parallelism": "replicas" if ws > 1 else "single",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single",
                    "l2": "inputs (268 MB each) larger than L2; no flush"},
-        "error_vs_fp64": err,
+        "error_vs_fp64": {**err, "reference": "FP64 product of the same inputs (torch float64 "
+                                               "matmul on the GPU)"},
         "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": n * n * 4},
-        "gpu_launches": args.steps,
+        "gpu_launches": launches,
         "roofline": roof,
         "clocks": clocks,
     }
+    if ffma is not None:
+        line["ffma"] = ffma
+        line["speedup_vs_ffma"] = value / ffma["value"]
+        line["error_ratio_vs_ffma"] = err["rel_fro"] / ffma["error_vs_fp64"]["rel_fro"]
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n)
     if rank == 0:
@@ -308,9 +377,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="ffma")
+    ap.add_argument("--variant", default="bf16x6",
+                    choices=["ffma", "bf16x3", "bf16x6", "bf16x3_scaled", "bf16x6_scaled"])
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FFMA comparison run")
+    ap.add_argument("--profile", action="store_true",
+                    help="timed steps only (no error check, e2e or CPU baseline): for ncu")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -5,6 +5,7 @@ package is the host-side interface over it (see sgemm.py).
 """
 from ._lib import (BF16X3, BF16X3_SCALED, BF16X6, BF16X6_SCALED, FFMA, VARIANTS,  # noqa: F401
                    HbsgError, LIB_PATH, lib)
-from .sgemm import gemm, gemm_workspace_size, sgemm, sgemm_workspace_size, tiles  # noqa: F401
+from .sgemm import (gemm, gemm_workspace_size, sgemm, sgemm_workspace_size,  # noqa: F401
+                    split_layout, tiles)
 
 __version__ = "1.0"

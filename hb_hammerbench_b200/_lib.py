@@ -35,13 +35,26 @@ VARIANTS = {"ffma": FFMA, "bf16x3": BF16X3, "bf16x6": BF16X6,
 class Config(ctypes.Structure):
     """struct hbsg_config"""
     _fields_ = [("tile", ctypes.c_int), ("split_k", ctypes.c_int),
-                ("raster_group", ctypes.c_int), ("chunk_k", ctypes.c_int)]
+                ("raster_group", ctypes.c_int), ("chunk_k", ctypes.c_int),
+                ("flags", ctypes.c_int)]
+
+
+FLAG_PRESPLIT_A = 1
+FLAG_PRESPLIT_B = 2
+FLAG_SPLIT_ONLY = 4
 
 
 class TileInfo(ctypes.Structure):
     """struct hbsg_tile_info"""
     _fields_ = [("variant_class", ctypes.c_int), ("bm", ctypes.c_int), ("bn", ctypes.c_int),
                 ("bk", ctypes.c_int), ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_int)]
+
+
+class SplitLayout(ctypes.Structure):
+    """struct hbsg_split_layout"""
+    _fields_ = [("parts", ctypes.c_int), ("kp", ctypes.c_int), ("a_offset", ctypes.c_size_t),
+                ("b_offset", ctypes.c_size_t), ("rowmax_offset", ctypes.c_size_t),
+                ("colmax_offset", ctypes.c_size_t), ("total_bytes", ctypes.c_size_t)]
 
 
 _P = ctypes.c_void_p
@@ -58,10 +71,12 @@ SIGNATURES = {
     "hbsg_gemm_ex": (_I, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _I,
                           ctypes.POINTER(Config), _P, _SZ, _P]),
     "hbsg_gemm_workspace_size": (_SZ, [_I, _I, _I, _I, ctypes.POINTER(Config)]),
+    "hbsg_get_split_layout": (_I, [_I, _I, _I, _I, ctypes.POINTER(SplitLayout)]),
     "hbsg_num_tiles": (_I, []),
     "hbsg_tile_describe": (_I, [_I, ctypes.POINTER(TileInfo)]),
     "hbsg_strerror": (ctypes.c_char_p, [_I]),
     "hbsg_check_device": (_I, [_P]),
+    "hbsg_debug_timeout_probe": (_I, [_P, _SZ, _P]),
     "hbsg_version": (_I, []),
 }
 

@@ -54,6 +54,44 @@ static int status_from(cudaError_t e) {
 
 static bool variant_valid(int v) { return v >= HBSG_FFMA && v <= HBSG_BF16X6_SCALED; }
 
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int parts_of(int variant) {
+  return (variant == HBSG_BF16X6 || variant == HBSG_BF16X6_SCALED) ? 3 : 2;
+}
+static bool scaled_of(int variant) {
+  return variant == HBSG_BF16X3_SCALED || variant == HBSG_BF16X6_SCALED;
+}
+
+// Workspace layout of the split-BF16 path (one problem; batches reuse it).
+struct SplitLayout {
+  int Kp;
+  size_t a_off, b_off, rowmax_off, colmax_off, total;
+};
+static SplitLayout split_layout(int M, int N, int K, int variant) {
+  SplitLayout L{};
+  const int P = parts_of(variant);
+  L.Kp = (K + 31) / 32 * 32;
+  if (L.Kp == 0) L.Kp = 32;
+  L.a_off = 0;
+  L.b_off = align256((size_t)P * M * L.Kp * 2);
+  L.rowmax_off = L.b_off + align256((size_t)P * N * L.Kp * 2);
+  L.colmax_off = L.rowmax_off + (scaled_of(variant) ? align256((size_t)M * 4) : 0);
+  L.total = L.colmax_off + (scaled_of(variant) ? align256((size_t)N * 4) : 0);
+  return L;
+}
+
+// Global tile ids: 1..F are the FFMA family, F+1..F+T the tensor-core family.
+static int total_tiles() { return ffma_num_tiles() + tc_num_tiles(); }
+
+static size_t workspace_needed(int M, int N, int K, int batch, int variant, const hbsg_config* cfg) {
+  if (variant == HBSG_FFMA) {
+    const int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
+    return ffma_workspace_bytes(M, N, batch, splits);
+  }
+  return split_layout(M, N, K, variant).total;
+}
+
 // Core dispatcher for one (possibly batched) GEMM.
 static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const float* A, long lda,
                          long strideA, const float* B, long ldb, long strideB, float* C, long ldc,
@@ -64,39 +102,89 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   if (M == 0 || N == 0 || batch == 0) return HBSG_OK;
   if (!C) return HBSG_ERR_INVALID_ARG;
   if (K > 0 && (!A || !B)) return HBSG_ERR_INVALID_ARG;
-  if (trans_a || trans_b) return HBSG_ERR_UNSUPPORTED;  // row-major only in this build
-  if (lda < (K > 0 ? K : 1) || ldb < N || ldc < N) return HBSG_ERR_INVALID_ARG;
+  // op(A) is M x K: stored M rows of K (row-major) or K rows of M (trans_a).
+  const long a_row = trans_a ? M : K;
+  const long b_row = trans_b ? K : N;
+  if (K > 0 && (lda < (a_row > 0 ? a_row : 1) || ldb < (b_row > 0 ? b_row : 1)))
+    return HBSG_ERR_INVALID_ARG;
+  if (ldc < N) return HBSG_ERR_INVALID_ARG;
   int dev = 0;
   const int sms = current_device_sms(&dev);
   if (sms < 0) return HBSG_ERR_NO_DEVICE;
-  if (variant != HBSG_FFMA) return HBSG_ERR_UNSUPPORTED;
 
   int tile = cfg && cfg->tile > 0 ? cfg->tile - 1 : -1;
-  if (tile >= ffma_num_tiles()) return HBSG_ERR_UNSUPPORTED;
-  if (tile < 0) tile = ffma_pick_tile(M, N, K, batch, sms);
-  int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
-  if (splits > 1 && K == 0) splits = 1;
-  const size_t need = ffma_workspace_bytes(M, N, batch, splits);
-  if (need > 0 && (!ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(ws) & 255)))
-    return HBSG_ERR_WORKSPACE;
+  if (tile >= total_tiles()) return HBSG_ERR_UNSUPPORTED;
 
-  FfmaParams p{};
-  p.A = A;
-  p.B = B;
-  p.C = C;
-  p.partial = static_cast<float*>(ws);
-  p.lda = lda;
-  p.ldb = ldb;
-  p.ldc = ldc;
-  p.strideA = strideA;
-  p.strideB = strideB;
-  p.strideC = strideC;
-  p.M = M;
-  p.N = N;
-  p.K = K;
-  p.splits = splits;
-  p.raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 8;
-  return status_from(ffma_launch(tile, p, batch, st));
+  if (variant == HBSG_FFMA) {
+    if (trans_a || trans_b) return HBSG_ERR_UNSUPPORTED;  // FFMA loaders are row-major only
+    if (tile >= ffma_num_tiles()) return HBSG_ERR_UNSUPPORTED;
+    if (tile < 0) tile = ffma_pick_tile(M, N, K, batch, sms);
+    int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
+    if (splits > 1 && K == 0) splits = 1;
+    const size_t need = ffma_workspace_bytes(M, N, batch, splits);
+    if (need > 0 && (!ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(ws) & 255)))
+      return HBSG_ERR_WORKSPACE;
+    FfmaParams p{};
+    p.A = A;
+    p.B = B;
+    p.C = C;
+    p.partial = static_cast<float*>(ws);
+    p.lda = lda;
+    p.ldb = ldb;
+    p.ldc = ldc;
+    p.strideA = strideA;
+    p.strideB = strideB;
+    p.strideC = strideC;
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.splits = splits;
+    p.raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 8;
+    return status_from(ffma_launch(tile, p, batch, st));
+  }
+
+  // ---- split-BF16 on the tensor cores ----
+  const int P = parts_of(variant);
+  const bool scaled = scaled_of(variant);
+  int tc = -1;
+  if (tile >= 0) {
+    tc = tile - ffma_num_tiles();
+    if (tc < 0 || tc_tile_parts(tc) != P) return HBSG_ERR_UNSUPPORTED;
+  } else {
+    tc = tc_pick_tile(M, N, P, sms);
+  }
+  if (cfg && cfg->split_k > 1) return HBSG_ERR_UNSUPPORTED;
+  const SplitLayout L = split_layout(M, N, K, variant);
+  if (!ws || ws_bytes < L.total || (reinterpret_cast<uintptr_t>(ws) & 255))
+    return HBSG_ERR_WORKSPACE;
+  uint8_t* w = static_cast<uint8_t*>(ws);
+  void* Ap = w + L.a_off;
+  void* Bp = w + L.b_off;
+  uint32_t* rowmax = scaled ? reinterpret_cast<uint32_t*>(w + L.rowmax_off) : nullptr;
+  uint32_t* colmax = scaled ? reinterpret_cast<uint32_t*>(w + L.colmax_off) : nullptr;
+  const int flags = cfg ? cfg->flags : 0;
+  const int raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 0;
+  const int chunk = cfg && cfg->chunk_k > 0 ? cfg->chunk_k : 0;
+  for (int b = 0; b < batch; ++b) {
+    const float* Ab = A + b * strideA;
+    const float* Bb = B + b * strideB;
+    float* Cb = C + b * strideC;
+    cudaError_t e = cudaSuccess;
+    if (!(flags & HBSG_FLAG_PRESPLIT_A)) {
+      e = trans_a ? split_operand_b(Ab, lda, K, M, L.Kp, P, scaled, Ap, rowmax, sms, st)
+                  : split_operand_a(Ab, lda, M, K, L.Kp, P, scaled, Ap, rowmax, sms, st);
+      if (e != cudaSuccess) return status_from(e);
+    }
+    if (!(flags & HBSG_FLAG_PRESPLIT_B)) {
+      e = trans_b ? split_operand_a(Bb, ldb, N, K, L.Kp, P, scaled, Bp, colmax, sms, st)
+                  : split_operand_b(Bb, ldb, K, N, L.Kp, P, scaled, Bp, colmax, sms, st);
+      if (e != cudaSuccess) return status_from(e);
+    }
+    if (flags & HBSG_FLAG_SPLIT_ONLY) continue;
+    e = tc_launch(tc, Ap, Bp, M, N, K, L.Kp, Cb, ldc, rowmax, colmax, raster, chunk, sms, 0, 0, st);
+    if (e != cudaSuccess) return status_from(e);
+  }
+  return HBSG_OK;
 }
 
 }  // namespace hbsg
@@ -126,10 +214,8 @@ int hbsg_sgemm_variant(const float* mat1, const float* mat2, float* result, int 
 }
 
 size_t hbsg_sgemm_workspace_size(int n, int niter, int variant) {
-  (void)n;
-  (void)niter;
-  (void)variant;
-  return 0;
+  if (n <= 0 || niter <= 0 || !variant_valid(variant)) return 0;
+  return workspace_needed(n, n, n, niter, variant, nullptr);
 }
 
 int hbsg_gemm(int trans_a, int trans_b, int m, int n, int k, const float* a, int64_t lda,
@@ -149,18 +235,33 @@ int hbsg_gemm_ex(int trans_a, int trans_b, int m, int n, int k, const float* a, 
 }
 
 size_t hbsg_gemm_workspace_size(int m, int n, int k, int variant, const hbsg_config* cfg) {
-  (void)k;
-  if (m <= 0 || n <= 0 || !variant_valid(variant)) return 0;
-  const int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
-  return ffma_workspace_bytes(m, n, 1, splits);
+  if (m <= 0 || n <= 0 || k < 0 || !variant_valid(variant)) return 0;
+  return workspace_needed(m, n, k, 1, variant, cfg);
 }
 
-int hbsg_num_tiles(void) { return ffma_num_tiles(); }
+int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* out) {
+  if (!out || m <= 0 || n <= 0 || k < 0) return HBSG_ERR_INVALID_ARG;
+  if (!variant_valid(variant) || variant == HBSG_FFMA) return HBSG_ERR_UNSUPPORTED;
+  const SplitLayout L = split_layout(m, n, k, variant);
+  out->parts = parts_of(variant);
+  out->kp = L.Kp;
+  out->a_offset = L.a_off;
+  out->b_offset = L.b_off;
+  out->rowmax_offset = scaled_of(variant) ? L.rowmax_off : L.total;
+  out->colmax_offset = scaled_of(variant) ? L.colmax_off : L.total;
+  out->total_bytes = L.total;
+  return HBSG_OK;
+}
+
+int hbsg_num_tiles(void) { return total_tiles(); }
 
 int hbsg_tile_describe(int tile, hbsg_tile_info* out) {
   if (!out) return HBSG_ERR_INVALID_ARG;
-  if (tile < 1 || tile > ffma_num_tiles()) return HBSG_ERR_INVALID_ARG;
-  return ffma_tile_info(tile - 1, out) ? HBSG_OK : HBSG_ERR_INVALID_ARG;
+  if (tile < 1 || tile > total_tiles()) return HBSG_ERR_INVALID_ARG;
+  const int idx = tile - 1;
+  const bool ok = idx < ffma_num_tiles() ? ffma_tile_info(idx, out)
+                                         : tc_tile_info(idx - ffma_num_tiles(), out);
+  return ok ? HBSG_OK : HBSG_ERR_INVALID_ARG;
 }
 
 const char* hbsg_strerror(int status) {
@@ -178,9 +279,30 @@ const char* hbsg_strerror(int status) {
 }
 
 int hbsg_check_device(hbsg_stream_t stream) {
+  if (current_device_sms(nullptr) < 0) return HBSG_ERR_NO_DEVICE;
   cudaError_t e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return status_from(e);
-  return HBSG_OK;
+  const int flag = read_and_clear_device_error();
+  return flag;
+}
+
+int hbsg_debug_timeout_probe(void* workspace, size_t workspace_bytes, hbsg_stream_t stream) {
+  if (!workspace || workspace_bytes < 65536 || (reinterpret_cast<uintptr_t>(workspace) & 255))
+    return HBSG_ERR_WORKSPACE;
+  const int sms = current_device_sms(nullptr);
+  if (sms < 0) return HBSG_ERR_NO_DEVICE;
+  // tiny problem: M = 128, N = 64, K = 32 on the 3-product, N = 64 tile
+  int tc = -1;
+  for (int i = 0; i < tc_num_tiles(); ++i) {
+    hbsg_tile_info info;
+    if (tc_tile_info(i, &info) && info.bn == 64 && tc_tile_parts(i) == 2) tc = i;
+  }
+  if (tc < 0) return HBSG_ERR_UNSUPPORTED;
+  uint8_t* w = static_cast<uint8_t*>(workspace);
+  cudaError_t e = tc_launch(tc, w, w + 16384, 128, 64, 32, 32, reinterpret_cast<float*>(w + 32768),
+                            64, nullptr, nullptr, 1, 32, sms, 1, 200000000ull,
+                            reinterpret_cast<cudaStream_t>(stream));
+  return status_from(e);
 }
 
 int hbsg_version(void) { return 100; }

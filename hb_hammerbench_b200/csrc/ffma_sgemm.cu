@@ -42,7 +42,10 @@ struct FfmaShape {
   static_assert(((AS / 4) & 1) == 1, "A pad keeps 8 rows in distinct bank groups");
 };
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC>
+// PAIR selects the packed two-lane FMA (__ffma2_rn, sm_100): each instruction
+// performs two independent IEEE fused multiply-adds, so the per-element
+// arithmetic is unchanged while half as many FMA instructions are issued.
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
 __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
     ffma_sgemm_kernel(FfmaParams p) {
   using S = FfmaShape<BM, BN, BK, WM, WN, STAGES>;
@@ -179,12 +182,27 @@ __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThread
 #pragma unroll
         for (int i = 0; i < TM; ++i) {
           const float av = k == 0 ? a4[i].x : k == 1 ? a4[i].y : k == 2 ? a4[i].z : a4[i].w;
+          if constexpr (PAIR) {
+            const float2 a2 = make_float2(av, av);
 #pragma unroll
-          for (int j = 0; j < TN / 4; ++j) {
-            acc[i][4 * j + 0] = __fmaf_rn(av, b4[j].x, acc[i][4 * j + 0]);
-            acc[i][4 * j + 1] = __fmaf_rn(av, b4[j].y, acc[i][4 * j + 1]);
-            acc[i][4 * j + 2] = __fmaf_rn(av, b4[j].z, acc[i][4 * j + 2]);
-            acc[i][4 * j + 3] = __fmaf_rn(av, b4[j].w, acc[i][4 * j + 3]);
+            for (int j = 0; j < TN / 4; ++j) {
+              float2 lo = __ffma2_rn(a2, make_float2(b4[j].x, b4[j].y),
+                                     make_float2(acc[i][4 * j + 0], acc[i][4 * j + 1]));
+              float2 hi = __ffma2_rn(a2, make_float2(b4[j].z, b4[j].w),
+                                     make_float2(acc[i][4 * j + 2], acc[i][4 * j + 3]));
+              acc[i][4 * j + 0] = lo.x;
+              acc[i][4 * j + 1] = lo.y;
+              acc[i][4 * j + 2] = hi.x;
+              acc[i][4 * j + 3] = hi.y;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < TN / 4; ++j) {
+              acc[i][4 * j + 0] = __fmaf_rn(av, b4[j].x, acc[i][4 * j + 0]);
+              acc[i][4 * j + 1] = __fmaf_rn(av, b4[j].y, acc[i][4 * j + 1]);
+              acc[i][4 * j + 2] = __fmaf_rn(av, b4[j].z, acc[i][4 * j + 2]);
+              acc[i][4 * j + 3] = __fmaf_rn(av, b4[j].w, acc[i][4 * j + 3]);
+            }
           }
         }
       }
@@ -250,11 +268,11 @@ struct FfmaEntry {
   cudaError_t (*launch)(const FfmaParams&, dim3, cudaStream_t, bool vec);
 };
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool PAIR>
 static cudaError_t launch_ffma(const FfmaParams& p, dim3 grid, cudaStream_t st, bool vec) {
   using S = FfmaShape<BM, BN, BK, WM, WN, STAGES>;
-  auto kv = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, true>;
-  auto ks = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false>;
+  auto kv = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, true, PAIR>;
+  auto ks = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, PAIR>;
   auto k = vec ? kv : ks;
   static uint32_t mask_v = 0, mask_s = 0;
   if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, vec ? &mask_v : &mask_s))
@@ -263,19 +281,23 @@ static cudaError_t launch_ffma(const FfmaParams& p, dim3 grid, cudaStream_t st, 
   return cudaGetLastError();
 }
 
-#define HBSG_FFMA_ENTRY(BM, BN, BK, WM, WN, ST)                                           \
-  FfmaEntry {                                                                             \
-    BM, BN, BK, WM, WN, ST, FfmaShape<BM, BN, BK, WM, WN, ST>::kThreads,                  \
-        FfmaShape<BM, BN, BK, WM, WN, ST>::kSmemBytes, &launch_ffma<BM, BN, BK, WM, WN, ST> \
+#define HBSG_FFMA_ENTRY(BM, BN, BK, WM, WN, ST, PAIR)                                   \
+  FfmaEntry {                                                                           \
+    BM, BN, BK, WM, WN, ST, FfmaShape<BM, BN, BK, WM, WN, ST>::kThreads,                \
+        FfmaShape<BM, BN, BK, WM, WN, ST>::kSmemBytes,                                  \
+        &launch_ffma<BM, BN, BK, WM, WN, ST, PAIR>                                      \
   }
 
 static const FfmaEntry kFfmaTiles[] = {
-    HBSG_FFMA_ENTRY(128, 256, 16, 64, 64, 4),  // 1: 8 warps, 128 FMA per thread per k
-    HBSG_FFMA_ENTRY(128, 128, 16, 64, 64, 4),  // 2: 4 warps
-    HBSG_FFMA_ENTRY(64, 64, 16, 32, 32, 4),    // 3: 4 warps, small problems
-    HBSG_FFMA_ENTRY(128, 64, 16, 64, 32, 4),   // 4: 4 warps, narrow N
-    HBSG_FFMA_ENTRY(128, 256, 32, 64, 64, 3),  // 5: 8 warps, deeper K tile
-    HBSG_FFMA_ENTRY(256, 128, 16, 64, 64, 4),  // 6: 8 warps, tall
+    HBSG_FFMA_ENTRY(128, 128, 16, 64, 64, 4, true),   // 1: 4 warps, 2 CTAs/SM, packed FMA
+    HBSG_FFMA_ENTRY(128, 256, 16, 64, 64, 4, true),   // 2: 8 warps, packed FMA
+    HBSG_FFMA_ENTRY(64, 64, 16, 32, 32, 4, true),     // 3: 4 warps, small problems
+    HBSG_FFMA_ENTRY(128, 64, 16, 64, 32, 4, true),    // 4: 4 warps, narrow N
+    HBSG_FFMA_ENTRY(128, 256, 32, 64, 64, 3, true),   // 5: 8 warps, deeper K tile
+    HBSG_FFMA_ENTRY(256, 128, 16, 64, 64, 4, true),   // 6: 8 warps, tall
+    HBSG_FFMA_ENTRY(128, 128, 32, 64, 64, 3, true),   // 7: 4 warps, deeper K tile
+    HBSG_FFMA_ENTRY(128, 128, 16, 64, 64, 4, false),  // 8: as 1 with scalar FMA
+    HBSG_FFMA_ENTRY(128, 256, 16, 64, 64, 4, false),  // 9: as 2 with scalar FMA
 };
 static constexpr int kNumFfmaTiles = sizeof(kFfmaTiles) / sizeof(kFfmaTiles[0]);
 
@@ -299,7 +321,7 @@ int ffma_pick_tile(int M, int N, int K, int batch, int num_sms) {
   (void)K;
   double best = -1.0;
   int best_idx = 0;
-  const int cand[] = {0, 1, 3, 2};
+  const int cand[] = {0, 1, 3, 2};  // 128x128, 128x256, 128x64, 64x64
   for (int idx : cand) {
     const FfmaEntry& e = kFfmaTiles[idx];
     const long tiles = (long)((M + e.bm - 1) / e.bm) * ((N + e.bn - 1) / e.bn) * batch;
@@ -308,7 +330,8 @@ int ffma_pick_tile(int M, int N, int K, int batch, int num_sms) {
     const double waves = tiles / slots;
     const double eff = waves / ceil(waves);  // tail efficiency
     // work per tile relative to the biggest tile: bigger tiles amortise loads
-    const double tile_eff = (e.bm * e.bn >= 128 * 256) ? 1.0 : (e.bm * e.bn >= 128 * 128 ? 0.93 : 0.8);
+    // measured at 8192^3: 128x128 (2 CTAs/SM) is the fastest shape
+    const double tile_eff = (e.bm * e.bn == 128 * 128) ? 1.0 : (e.bm * e.bn >= 128 * 256 ? 0.96 : 0.85);
     const double fill = fmin(1.0, tiles / slots);
     const double score = eff * tile_eff * (fill < 1.0 ? fill : 1.0);
     if (score > best + 1e-9) {

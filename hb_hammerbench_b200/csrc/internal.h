@@ -31,6 +31,21 @@ int ffma_pick_tile(int M, int N, int K, int batch, int num_sms);
 size_t ffma_workspace_bytes(int M, int N, int batch, int splits);
 cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st);
 
+// ---- split-BF16 family ----------------------------------------------------------
+cudaError_t split_operand_a(const float* A, long lda, int M, int K, int Kp, int parts, bool scaled,
+                            void* Ap, uint32_t* rowmax, int sms, cudaStream_t st);
+cudaError_t split_operand_b(const float* B, long ldb, int K, int N, int Kp, int parts, bool scaled,
+                            void* Bp, uint32_t* colmax, int sms, cudaStream_t st);
+int tc_num_tiles();
+bool tc_tile_info(int idx, hbsg_tile_info* out);
+int tc_tile_parts(int idx);
+int tc_pick_tile(int M, int N, int parts, int sms);
+cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,
+                      float* C, long ldc, const uint32_t* rowmax, const uint32_t* colmax,
+                      int raster, int chunk_k, int sms, int debug_skip_loads,
+                      unsigned long long wait_limit_ns, cudaStream_t st);
+int read_and_clear_device_error();
+
 // ---- device state -------------------------------------------------------------
 // Returns the SM count of the current device (cached per device), or -1 when
 // no sm_100 device is current.

@@ -126,6 +126,14 @@ def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, varian
     return c
 
 
+def split_layout(m: int, n: int, k: int, variant="bf16x6") -> dict:
+    """Byte offsets of the BF16 operand parts inside a split-BF16 workspace."""
+    lay = _lib.SplitLayout()
+    check(lib().hbsg_get_split_layout(m, n, k, _variant(variant), ctypes.byref(lay)),
+          "hbsg_get_split_layout")
+    return {f: getattr(lay, f) for f, _ in _lib.SplitLayout._fields_}
+
+
 def tiles() -> list[dict]:
     """The tile-shape table (1-based ids) the autotuner searches."""
     out = []

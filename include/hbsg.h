@@ -54,7 +54,18 @@ typedef struct hbsg_config {
     int raster_group;  /* tile rows per rasterisation group (0 = heuristic) */
     int chunk_k;       /* split-BF16: K elements accumulated on the tensor core before the
                           partial is added in FP32 registers (0 = heuristic) */
+    int flags;         /* HBSG_FLAG_* */
 } hbsg_config;
+
+/* hbsg_config.flags. PRESPLIT_A / PRESPLIT_B: the workspace already holds the
+ * BF16 split of A / B made by an earlier call with the same operand values,
+ * shape, transpose flag, variant and workspace (e.g. a constant operand), so
+ * the split pass for it is skipped. */
+#define HBSG_FLAG_PRESPLIT_A 1
+#define HBSG_FLAG_PRESPLIT_B 2
+/* SPLIT_ONLY: run only the split passes (fill the workspace), no product;
+ * a later call with PRESPLIT_A | PRESPLIT_B computes C from them. */
+#define HBSG_FLAG_SPLIT_ONLY 4
 
 typedef struct hbsg_tile_info {
     int variant_class; /* 0 = FFMA kernel family, 1 = split-BF16 tensor-core family */
@@ -111,6 +122,20 @@ int hbsg_gemm_ex(int trans_a, int trans_b, int m, int n, int k,
 size_t hbsg_gemm_workspace_size(int m, int n, int k, int variant,
                                 const hbsg_config* cfg);
 
+/* Where the split-BF16 path keeps the operand parts inside its workspace
+ * (byte offsets from the workspace start). Parts are BF16, K-major:
+ *   A parts: [parts][m][kp] at a_offset   (op(A) rows, K padded to kp with zeros)
+ *   B parts: [parts][n][kp] at b_offset   (op(B) columns, transposed)
+ *   rowmax / colmax: m / n uint32 FP32 bit patterns of max|row| / max|column|
+ *   (scaled variants only; offsets equal total_bytes otherwise).
+ * Part 0 = hi, 1 = mid, 2 = lo. */
+typedef struct hbsg_split_layout {
+    int parts;
+    int kp;
+    size_t a_offset, b_offset, rowmax_offset, colmax_offset, total_bytes;
+} hbsg_split_layout;
+int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* out);
+
 /* Tile-shape table for the autotuner: number of ids and their description. */
 int hbsg_num_tiles(void);
 int hbsg_tile_describe(int tile, hbsg_tile_info* out);
@@ -123,6 +148,14 @@ const char* hbsg_strerror(int status);
 /* Synchronises `stream`, then reports and clears the device-side error flag
  * raised by bounded waits inside the kernels (HBSG_OK if none). */
 int hbsg_check_device(hbsg_stream_t stream);
+
+/* Test hook for the failure path of the tensor-core kernel: launches it on a
+ * tiny problem with its tile loads suppressed and a 0.2 s bound on every
+ * wait, so the waits expire, the kernel records HBSG_ERR_DEVICE_TIMEOUT,
+ * releases its tensor memory and returns. `workspace` (>= 64 KiB, 256-byte
+ * aligned) only backs the tensor maps; nothing is read or written. The next
+ * hbsg_check_device reports the timeout. No reference counterpart. */
+int hbsg_debug_timeout_probe(void* workspace, size_t workspace_bytes, hbsg_stream_t stream);
 
 /* ABI version (major * 100 + minor). */
 int hbsg_version(void);

@@ -1,0 +1,235 @@
+"""Split-BF16 tensor-core path on the GPU, called through the C ABI.
+
+Bars:
+  - integer fixtures of the reference (i%7 / i%3, ramp x identity): bit-exact
+    for every variant (small integers split exactly and sum exactly);
+  - the split pre-pass: bit-exact against the oracle's split (oracle.c);
+  - floating point: error vs the FP64 product no worse than the FFMA kernel's
+    for the 6-product forms at K >= 512, and within
+    stated bounds otherwise.
+"""
+import ctypes
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = ["bf16x3", "bf16x6", "bf16x3_scaled", "bf16x6_scaled"]
+
+
+@pytest.fixture(scope="module")
+def hb():
+    import hb_hammerbench_b200 as hb
+    return hb
+
+
+def _dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+
+
+def _err(C, ref):
+    import torch
+    d = C.double() - ref
+    return float(torch.linalg.norm(d) / torch.linalg.norm(ref)), float(d.abs().max())
+
+
+def _rand(shape, seed, wide=False):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.rand(shape, device="cuda", generator=g) * 2 - 1
+    if wide:
+        u = torch.rand(shape, device="cuda", generator=g) * 40 - 20
+        x = torch.sign(x) * torch.exp2(u)
+    return x
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_reference_fixture_bit_exact(hb, oracle_mod, golden_dir, variant):
+    fix = json.load(open(os.path.join(golden_dir, "sgemm_mod_N512_NITER2.json")))
+    n, niter = fix["N"], fix["NITER"]
+    m1, m2 = oracle_mod.fill_mod(niter * n * n)
+    out = hb.sgemm(_dev(m1), _dev(m2), n=n, niter=niter, variant=variant).cpu().numpy()
+    assert hashlib.sha256(out.tobytes()).hexdigest() == fix["sha256_result_f32"]
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x6_scaled"])
+def test_ramp_identity_exact(hb, oracle_mod, variant):
+    a, b = oracle_mod.fill_ramp_identity(512)  # A[i] = i needs all three parts
+    out = hb.gemm(_dev(a), _dev(b), variant=variant).cpu().numpy()
+    assert np.array_equal(out, a)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("m,n,k,trans", [(200, 136, 100, (0, 0)), (77, 300, 65, (1, 0)),
+                                         (130, 70, 96, (0, 1)), (64, 64, 40, (1, 1))])
+def test_split_pass_bit_exact(hb, oracle_mod, variant, m, n, k, trans):
+    import torch
+    ta, tb = trans
+    wide = "scaled" in variant
+    rng = np.random.Generator(np.random.PCG64(m * n + k))
+    A = rng.uniform(-1, 1, (m, k)).astype(np.float32)
+    B = rng.uniform(-1, 1, (k, n)).astype(np.float32)
+    if wide:
+        A *= np.exp2(rng.uniform(-20, 20, A.shape)).astype(np.float32)
+        B *= np.exp2(rng.uniform(-20, 20, B.shape)).astype(np.float32)
+    a_st = np.ascontiguousarray(A.T) if ta else A
+    b_st = np.ascontiguousarray(B.T) if tb else B
+    lay = hb.split_layout(m, n, k, variant)
+    ws = torch.zeros(lay["total_bytes"], dtype=torch.uint8, device="cuda")
+    hb.gemm(_dev(a_st), _dev(b_st), variant=variant, trans_a=bool(ta), trans_b=bool(tb), workspace=ws)
+    w = ws.cpu().numpy()
+    P, kp = lay["parts"], lay["kp"]
+    ap = w[lay["a_offset"]:lay["a_offset"] + P * m * kp * 2].view(np.uint16).reshape(P, m, kp)
+    bp = w[lay["b_offset"]:lay["b_offset"] + P * n * kp * 2].view(np.uint16).reshape(P, n, kp)
+    for i in range(m):
+        e = oracle_mod.pow2_exponent(A[i]) if wide else 0
+        parts = oracle_mod.split_bf16(A[i], e, P)
+        for p in range(P):
+            assert np.array_equal(ap[p, i, :k], parts[p]), (i, p)
+    assert not ap[:, :, k:].any()
+    for j in range(n):
+        e = oracle_mod.pow2_exponent(B[:, j]) if wide else 0
+        parts = oracle_mod.split_bf16(B[:, j], e, P)
+        for p in range(P):
+            assert np.array_equal(bp[p, j, :k], parts[p]), (j, p)
+    if wide:
+        rm = w[lay["rowmax_offset"]:lay["rowmax_offset"] + 4 * m].view(np.float32)
+        assert np.array_equal(rm, np.abs(A).max(axis=1))
+
+
+@pytest.mark.parametrize("m,n,k", [(1024, 1024, 1024), (768, 1280, 4096), (512, 512, 8192)])
+def test_x6_error_not_worse_than_ffma(hb, m, n, k):
+    A = _rand((m, k), m + k)
+    B = _rand((k, n), n + k + 1)
+    ref = A.double() @ B.double()
+    e_ffma = _err(hb.gemm(A, B), ref)
+    for v in ("bf16x6", "bf16x6_scaled"):
+        e = _err(hb.gemm(A, B, variant=v), ref)
+        assert e[0] <= e_ffma[0], (v, e, e_ffma)
+        assert e[1] <= 1.5 * e_ffma[1], (v, e, e_ffma)
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (33, 65, 17), (300, 7, 129), (129, 257, 31), (640, 96, 2000)])
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_ragged_shapes_error_bounds(hb, m, n, k, variant):
+    A = _rand((m, k), m * 7 + k)
+    B = _rand((k, n), n * 5 + k)
+    ref = A.double() @ B.double()
+    e_ffma = _err(hb.gemm(A, B), ref)
+    e = _err(hb.gemm(A, B, variant=variant), ref)
+    # 3-product: 2-part split holds ~16 bits; 6-product: within 3x FFMA at short K
+    bound = 2.0 ** -16 if "x3" in variant else max(3 * e_ffma[0], 2.0 ** -23)
+    assert e[0] <= bound, (e, e_ffma)
+
+
+@pytest.mark.parametrize("trans", [(1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
+def test_transposed_operands(hb, trans, variant):
+    import torch
+    m, n, k = 300, 200, 520
+    A = _rand((m, k), 11)
+    B = _rand((k, n), 12)
+    ref = A.double() @ B.double()
+    a = A.t().contiguous() if trans[0] else A
+    b = B.t().contiguous() if trans[1] else B
+    C = hb.gemm(a, b, variant=variant, trans_a=bool(trans[0]), trans_b=bool(trans[1]))
+    C0 = hb.gemm(A, B, variant=variant)
+    assert torch.equal(C, C0)  # same split values, same kernel: identical bits
+    assert _err(C, ref)[0] < (2.0 ** -16 if "x3" in variant else 2e-6)
+
+
+def test_wide_range_scaled_not_worse_than_ffma(hb):
+    n = 1024
+    A = _rand((n, n), 21, wide=True)
+    B = _rand((n, n), 22, wide=True)
+    ref = A.double() @ B.double()
+    e_ffma = _err(hb.gemm(A, B), ref)
+    e = _err(hb.gemm(A, B, variant="bf16x6_scaled"), ref)
+    assert e[0] <= e_ffma[0], (e, e_ffma)
+
+
+def test_range_extremes_need_scaling(hb):
+    # |A| ~ 2^-120: the unscaled mid/lo parts fall below the normal BF16 range;
+    # the scaled form works at row scale 2^0 and keeps full accuracy.
+    import torch
+    n = 256
+    A = _rand((n, n), 31) * 2.0 ** -120
+    B = _rand((n, n), 32) * 2.0 ** 100
+    ref = A.double() @ B.double()
+    e_ffma = _err(hb.gemm(A, B), ref)
+    e_s = _err(hb.gemm(A, B, variant="bf16x6_scaled"), ref)
+    assert e_s[0] <= 3 * e_ffma[0] + 1e-12, (e_s, e_ffma)
+
+
+def test_presplit_reuse_and_determinism(hb):
+    import torch
+    m, n, k = 512, 384, 768
+    A = _rand((m, k), 41)
+    B = _rand((k, n), 42)
+    ws = torch.empty(hb.gemm_workspace_size(m, n, k, "bf16x6"), dtype=torch.uint8, device="cuda")
+    C1 = hb.gemm(A, B, variant="bf16x6", workspace=ws)
+    C2 = hb.gemm(A, B, variant="bf16x6", workspace=ws)
+    C3 = hb.gemm(A, B, variant="bf16x6", workspace=ws, config={"flags": 3})
+    assert torch.equal(C1, C2) and torch.equal(C1, C3)
+    # constant B: only A is re-split
+    A2 = _rand((m, k), 43)
+    C4 = hb.gemm(A2, B, variant="bf16x6", workspace=ws, config={"flags": 2})
+    assert torch.equal(C4, hb.gemm(A2, B, variant="bf16x6"))
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x6_scaled"])
+def test_batched_matches_single(hb, variant):
+    import torch
+    n, niter = 256, 3
+    A = _rand((niter, n, n), 51)
+    B = _rand((niter, n, n), 52)
+    C = hb.sgemm(A, B, n=n, niter=niter, variant=variant)
+    for i in range(niter):
+        assert torch.equal(C[i], hb.gemm(A[i], B[i], variant=variant))
+
+
+def test_strided_output(hb):
+    import torch
+    m, n, k = 200, 150, 300
+    A = _rand((m, k), 61)
+    B = _rand((k, n), 62)
+    buf = torch.full((m, n + 9), float("nan"), device="cuda")
+    c = buf[:, 3:n + 3]
+    hb.gemm(A, B, c, variant="bf16x6_scaled")
+    assert torch.equal(c, hb.gemm(A, B, variant="bf16x6_scaled"))
+    assert torch.isnan(buf[:, :3]).all() and torch.isnan(buf[:, n + 3:]).all()
+
+
+@pytest.mark.parametrize("tile", [10, 11, 12, 13, 14, 15])
+def test_every_tensor_core_tile(hb, tile):
+    info = [t for t in hb.tiles() if t["tile"] == tile][0]
+    assert info["family"] == "bf16"
+    m, n, k = 300, 520, 256
+    A = _rand((m, k), tile)
+    B = _rand((k, n), tile + 100)
+    ref = A.double() @ B.double()
+    for v in ("bf16x6", "bf16x3"):
+        try:
+            C = hb.gemm(A, B, variant=v, config={"tile": tile})
+        except hb.HbsgError as e:
+            assert e.status == -2  # tile belongs to the other product count
+            continue
+        assert _err(C, ref)[0] < (2.0 ** -16 if v == "bf16x3" else 2e-6)
+
+
+def test_device_wait_timeout_is_reported_and_recoverable(hb):
+    import torch
+    from hb_hammerbench_b200 import _lib
+    ws = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
+    st = _lib.lib().hbsg_debug_timeout_probe(ctypes.c_void_p(ws.data_ptr()), 1 << 20, None)
+    assert st == _lib.OK
+    assert _lib.lib().hbsg_check_device(None) == _lib.ERR_DEVICE_TIMEOUT
+    assert _lib.lib().hbsg_check_device(None) == _lib.OK  # flag cleared
+    A = _rand((256, 256), 71)
+    B = _rand((256, 256), 72)
+    assert _err(hb.gemm(A, B, variant="bf16x6"), A.double() @ B.double())[0] < 2e-6
