@@ -42,6 +42,7 @@ class Config(ctypes.Structure):
 FLAG_PRESPLIT_A = 1
 FLAG_PRESPLIT_B = 2
 FLAG_SPLIT_ONLY = 4
+NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024  # HBSG_NOALLOC_SCRATCH_BYTES
 
 
 class TileInfo(ctypes.Structure):
@@ -72,6 +73,7 @@ SIGNATURES = {
                           ctypes.POINTER(Config), _P, _SZ, _P]),
     "hbsg_gemm_workspace_size": (_SZ, [_I, _I, _I, _I, ctypes.POINTER(Config)]),
     "hbsg_get_split_layout": (_I, [_I, _I, _I, _I, ctypes.POINTER(SplitLayout)]),
+    "hbsg_gemm_noalloc": (_I, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _I, _P]),
     "hbsg_num_tiles": (_I, []),
     "hbsg_tile_describe": (_I, [_I, ctypes.POINTER(TileInfo)]),
     "hbsg_strerror": (ctypes.c_char_p, [_I]),

@@ -136,6 +136,38 @@ typedef struct hbsg_split_layout {
 } hbsg_split_layout;
 int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* out);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free split-BF16 GEMM. No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory at the moment they need a
+ * product: applications whose memory pool has already reserved (nearly) all
+ * of the GPU, so a workspace allocation would fail or force the pool to
+ * release memory; and latency-critical loops, where cudaMalloc/cudaFree may
+ * synchronise the device and stall every stream. Same arguments and result
+ * as hbsg_gemm with a split-BF16 variant (BF16X3, BF16X6 and their _SCALED
+ * forms), but the split parts live in a fixed scratch array compiled into
+ * the library: HBSG_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory that
+ * every GPU which loads the library holds until the process exits.
+ *
+ *   - Problems whose split workspace (hbsg_get_split_layout().total_bytes)
+ *     exceeds HBSG_NOALLOC_SCRATCH_BYTES are rejected with
+ *     HBSG_ERR_WORKSPACE before anything is launched. M = N = K = 1024 with
+ *     BF16X6 needs 12.6 MB and fits.
+ *   - FFMA is rejected with HBSG_ERR_UNSUPPORTED (it needs no scratch: call
+ *     hbsg_gemm).
+ *   - The first call on each device looks up the array's device address
+ *     (set-up, no allocation); make that first call before any stream
+ *     capture begins.
+ *   - All calls on a device share the one array: calls that may overlap on
+ *     the GPU (different streams without ordering between them) race on it
+ *     and must be serialised by the caller. Nothing needs clearing between
+ *     calls: each call rewrites every scratch byte it later reads.
+ */
+#define HBSG_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int hbsg_gemm_noalloc(int trans_a, int trans_b, int m, int n, int k,
+                      const float* a, int64_t lda, const float* b, int64_t ldb,
+                      float* c, int64_t ldc, int variant, hbsg_stream_t stream);
+
 /* Tile-shape table for the autotuner: number of ids and their description. */
 int hbsg_num_tiles(void);
 int hbsg_tile_describe(int tile, hbsg_tile_info* out);
