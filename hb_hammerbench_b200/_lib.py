@@ -58,6 +58,14 @@ class SplitLayout(ctypes.Structure):
                 ("colmax_offset", ctypes.c_size_t), ("total_bytes", ctypes.c_size_t)]
 
 
+class Problem(ctypes.Structure):
+    """struct hbsg_problem"""
+    _fields_ = [("m", ctypes.c_int), ("n", ctypes.c_int), ("k", ctypes.c_int),
+                ("a", ctypes.c_void_p), ("lda", ctypes.c_int64),
+                ("b", ctypes.c_void_p), ("ldb", ctypes.c_int64),
+                ("c", ctypes.c_void_p), ("ldc", ctypes.c_int64)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -74,6 +82,12 @@ SIGNATURES = {
     "hbsg_gemm_workspace_size": (_SZ, [_I, _I, _I, _I, ctypes.POINTER(Config)]),
     "hbsg_get_split_layout": (_I, [_I, _I, _I, _I, ctypes.POINTER(SplitLayout)]),
     "hbsg_gemm_noalloc": (_I, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _I, _P]),
+    "hbsg_grouped_workspace_size": (_SZ, [_I, ctypes.POINTER(Problem), _I, ctypes.POINTER(Config)]),
+    "hbsg_grouped_plan_create": (_I, [ctypes.POINTER(_P), _I, ctypes.POINTER(Problem), _I,
+                                      ctypes.POINTER(Config), _P, _SZ]),
+    "hbsg_grouped_run": (_I, [_P, _P]),
+    "hbsg_grouped_plan_destroy": (_I, [_P]),
+    "hbsg_gemm_grouped": (_I, [_I, ctypes.POINTER(Problem), _I, ctypes.POINTER(Config), _P, _SZ, _P]),
     "hbsg_num_tiles": (_I, []),
     "hbsg_tile_describe": (_I, [_I, ctypes.POINTER(TileInfo)]),
     "hbsg_strerror": (ctypes.c_char_p, [_I]),

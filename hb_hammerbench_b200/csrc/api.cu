@@ -282,8 +282,9 @@ int hbsg_check_device(hbsg_stream_t stream) {
   if (current_device_sms(nullptr) < 0) return HBSG_ERR_NO_DEVICE;
   cudaError_t e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return status_from(e);
-  const int flag = read_and_clear_device_error();
-  return flag;
+  const int f1 = tc_read_and_clear_device_error();
+  const int f2 = grouped_read_and_clear_device_error();
+  return f1 != HBSG_OK ? f1 : f2;
 }
 
 int hbsg_debug_timeout_probe(void* workspace, size_t workspace_bytes, hbsg_stream_t stream) {

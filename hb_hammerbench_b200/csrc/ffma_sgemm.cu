@@ -21,43 +21,14 @@
 // (tm, tn) owns rows {tm + 8i} and columns {16j + 4tn + c} of its warp tile:
 // a quarter-warp reads 8 distinct A rows (no conflict) and one B float4
 // (broadcast); the whole warp reads 64 contiguous bytes of B.
-#include "common.cuh"
-#include "internal.h"
+#include "ffma_kernel.cuh"
 
 namespace hbsg {
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
-struct FfmaShape {
-  static constexpr int kWarpsM = BM / WM;
-  static constexpr int kWarpsN = BN / WN;
-  static constexpr int kThreads = kWarpsM * kWarpsN * 32;
-  static constexpr int TM = WM / 8;
-  static constexpr int TN = WN / 4;
-  static constexpr int AS = BK + 4;
-  static constexpr int kAStage = BM * AS;
-  static constexpr int kBStage = BK * BN;
-  static constexpr int kSmemBytes = STAGES * (kAStage + kBStage) * 4;
-  static_assert(WM % 8 == 0 && WN % 16 == 0, "warp tile");
-  static_assert(BK % 4 == 0, "BK");
-  static_assert(((AS / 4) & 1) == 1, "A pad keeps 8 rows in distinct bank groups");
-};
-
-// PAIR selects the packed two-lane FMA (__ffma2_rn, sm_100): each instruction
-// performs two independent IEEE fused multiply-adds, so the per-element
-// arithmetic is unchanged while half as many FMA instructions are issued.
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
 __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
     ffma_sgemm_kernel(FfmaParams p) {
-  using S = FfmaShape<BM, BN, BK, WM, WN, STAGES>;
-  constexpr int NT = S::kThreads;
-  constexpr int TM = S::TM;
-  constexpr int TN = S::TN;
-  constexpr int AS = S::AS;
-
   extern __shared__ __align__(16) float smem[];
-  float* As = smem;
-  float* Bs = smem + STAGES * S::kAStage;
-
   // Rasterised tile order: groups of `raster` tile rows, column-major inside
   // a group, so CTAs resident at the same time share A and B strips in L2.
   const int t = blockIdx.x;
@@ -66,179 +37,27 @@ __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThread
   const int first_m = group * p.raster;
   const int gm = min(p.raster, p.tiles_m - first_m);
   const int in_group = t - group * group_span;
-  const int tile_m = first_m + in_group % gm;
-  const int tile_n = in_group / gm;
-  const int m0 = tile_m * BM;
-  const int n0 = tile_n * BN;
-
+  const int m0 = (first_m + in_group % gm) * BM;
+  const int n0 = (in_group / gm) * BN;
   const int batch = blockIdx.z;
   const int split = blockIdx.y;
-  const float* __restrict__ A = p.A + batch * p.strideA;
-  const float* __restrict__ B = p.B + batch * p.strideB;
-
   const int k_begin = split * p.k_per_split;
   const int k_end = min(p.K, k_begin + p.k_per_split);
-  const int KT = k_end > k_begin ? (k_end - k_begin + BK - 1) / BK : 0;
-
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
-  const int wm = warp / S::kWarpsN;
-  const int wn = warp % S::kWarpsN;
-  const int tm = lane & 7;
-  const int tn = lane >> 3;
-
-  auto load_tile = [&](int slot, int kt) {
-    const int k0 = k_begin + kt * BK;
-    float* as = As + slot * S::kAStage;
-    float* bs = Bs + slot * S::kBStage;
-    if constexpr (VEC) {
-      constexpr int ACH = BM * BK / 4;
-#pragma unroll
-      for (int c = tid; c < ACH; c += NT) {
-        const int r = c / (BK / 4);
-        const int kc = (c % (BK / 4)) * 4;
-        const int gr = m0 + r;
-        const int gk = k0 + kc;
-        int bytes = 0;
-        const float* src = A;
-        if (gr < p.M && gk < k_end) {
-          bytes = min(4, k_end - gk) * 4;
-          src = A + (long)gr * p.lda + gk;
-        }
-        cp_async16(as + r * AS + kc, src, bytes);
-      }
-      constexpr int BCH = BK * BN / 4;
-#pragma unroll
-      for (int c = tid; c < BCH; c += NT) {
-        const int r = c / (BN / 4);
-        const int nc = (c % (BN / 4)) * 4;
-        const int gk = k0 + r;
-        const int gn = n0 + nc;
-        int bytes = 0;
-        const float* src = B;
-        if (gk < k_end && gn < p.N) {
-          bytes = min(4, p.N - gn) * 4;
-          src = B + (long)gk * p.ldb + gn;
-        }
-        cp_async16(bs + r * BN + nc, src, bytes);
-      }
-    } else {
-#pragma unroll 4
-      for (int c = tid; c < BM * BK; c += NT) {
-        const int r = c / BK;
-        const int kc = c % BK;
-        const int gr = m0 + r;
-        const int gk = k0 + kc;
-        const bool ok = gr < p.M && gk < k_end;
-        cp_async4(as + r * AS + kc, ok ? A + (long)gr * p.lda + gk : A, ok ? 4 : 0);
-      }
-#pragma unroll 4
-      for (int c = tid; c < BK * BN; c += NT) {
-        const int r = c / BN;
-        const int nc = c % BN;
-        const int gk = k0 + r;
-        const int gn = n0 + nc;
-        const bool ok = gk < k_end && gn < p.N;
-        cp_async4(bs + r * BN + nc, ok ? B + (long)gk * p.ldb + gn : B, ok ? 4 : 0);
-      }
-    }
-  };
-
-  float acc[TM][TN];
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
-
-#pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < KT) load_tile(s, s);
-    cp_async_commit();
-  }
-
-  for (int kt = 0; kt < KT; ++kt) {
-    cp_async_wait<STAGES - 2>();
-    __syncthreads();
-    {
-      const int nk = kt + STAGES - 1;
-      if (nk < KT) load_tile(nk % STAGES, nk);
-      cp_async_commit();
-    }
-    const int slot = kt % STAGES;
-    const float* a_s = As + slot * S::kAStage + (wm * WM + tm) * AS;
-    const float* b_s = Bs + slot * S::kBStage + wn * WN + 4 * tn;
-#pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      float4 a4[TM];
-#pragma unroll
-      for (int i = 0; i < TM; ++i) a4[i] = *reinterpret_cast<const float4*>(a_s + i * 8 * AS + kk);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        float4 b4[TN / 4];
-#pragma unroll
-        for (int j = 0; j < TN / 4; ++j)
-          b4[j] = *reinterpret_cast<const float4*>(b_s + (kk + k) * BN + 16 * j);
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-          const float av = k == 0 ? a4[i].x : k == 1 ? a4[i].y : k == 2 ? a4[i].z : a4[i].w;
-          if constexpr (PAIR) {
-            const float2 a2 = make_float2(av, av);
-#pragma unroll
-            for (int j = 0; j < TN / 4; ++j) {
-              float2 lo = __ffma2_rn(a2, make_float2(b4[j].x, b4[j].y),
-                                     make_float2(acc[i][4 * j + 0], acc[i][4 * j + 1]));
-              float2 hi = __ffma2_rn(a2, make_float2(b4[j].z, b4[j].w),
-                                     make_float2(acc[i][4 * j + 2], acc[i][4 * j + 3]));
-              acc[i][4 * j + 0] = lo.x;
-              acc[i][4 * j + 1] = lo.y;
-              acc[i][4 * j + 2] = hi.x;
-              acc[i][4 * j + 3] = hi.y;
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < TN / 4; ++j) {
-              acc[i][4 * j + 0] = __fmaf_rn(av, b4[j].x, acc[i][4 * j + 0]);
-              acc[i][4 * j + 1] = __fmaf_rn(av, b4[j].y, acc[i][4 * j + 1]);
-              acc[i][4 * j + 2] = __fmaf_rn(av, b4[j].z, acc[i][4 * j + 2]);
-              acc[i][4 * j + 3] = __fmaf_rn(av, b4[j].w, acc[i][4 * j + 3]);
-            }
-          }
-        }
-      }
-    }
-  }
-  cp_async_wait<0>();
-
-  // Epilogue: direct stores (split-K slices go to the partial buffer).
   float* C;
   long ldc;
-  if (p.splits > 1) {
+  bool vec_store;
+  if (p.splits > 1) {  // split-K slices go to the partial buffer
     C = p.partial + ((long)batch * p.splits + split) * (long)p.M * p.N;
     ldc = p.N;
+    vec_store = (p.N & 3) == 0;
   } else {
     C = p.C + batch * p.strideC;
     ldc = p.ldc;
+    vec_store = p.vec_store;
   }
-  const bool vec_store = p.splits > 1 ? ((p.N & 3) == 0) : p.vec_store;
-#pragma unroll
-  for (int i = 0; i < TM; ++i) {
-    const int r = m0 + wm * WM + tm + 8 * i;
-    if (r >= p.M) continue;
-    float* crow = C + (long)r * ldc;
-#pragma unroll
-    for (int j = 0; j < TN / 4; ++j) {
-      const int c = n0 + wn * WN + 16 * j + 4 * tn;
-      if (vec_store && c + 3 < p.N) {
-        *reinterpret_cast<float4*>(crow + c) =
-            make_float4(acc[i][4 * j], acc[i][4 * j + 1], acc[i][4 * j + 2], acc[i][4 * j + 3]);
-      } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (c + e < p.N) crow[c + e] = acc[i][4 * j + e];
-      }
-    }
-  }
+  ffma_tile<BM, BN, BK, WM, WN, STAGES, VEC, PAIR>(p.A + batch * p.strideA, p.lda,
+                                                   p.B + batch * p.strideB, p.ldb, p.M, p.N,
+                                                   k_begin, k_end, m0, n0, C, ldc, vec_store, smem);
 }
 
 // Fixed-order reduction of split-K partial slices: C = ((p0 + p1) + p2) + ...

@@ -1,0 +1,639 @@
+// Grouped SGEMM: many independent FP32 GEMMs of uneven M, N, K in one
+// persistent launch, captured with its split passes in one CUDA graph.
+//
+// The reference's only multi-GEMM form is the NITER loop of independent
+// products (apps/sgemm/kernel.cpp:293-297) over equal sizes, and its legacy
+// cooperative kernel strides tile groups over the output grid
+// (apps/legacy/gemm/sgemm_group_cooperative/kernel.cpp:285-286). Here the
+// output tiles of all problems form one list:
+//   - problems are ordered by K (the cost of a tile) descending, and each
+//     problem's tiles are listed in rasterised order;
+//   - CTA b of the persistent grid takes tiles b, b + G, b + 2G, ...
+// so the ~G tiles in flight at any moment have similar cost (balanced waves)
+// and mostly belong to one or two problems (their operand strips are shared
+// in L2).
+//
+// Split-BF16 forms: one grouped split pass over all problems writes every
+// problem's BF16 parts into the workspace; the tensor-core kernel body
+// (tc_kernel.cuh) then runs over the tile list with two TMA tensor maps per
+// problem kept in global memory. FFMA: the FFMA tile body (ffma_kernel.cuh)
+// runs over the tile list.
+//
+// A plan (hbsg_grouped_plan_create) lays the tables out in the caller's
+// workspace, uploads them once, and captures the launches into a CUDA graph;
+// hbsg_grouped_run replays that graph on a stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "ffma_kernel.cuh"
+#include "split_kernel.cuh"
+#include "tc_kernel.cuh"
+
+namespace hbsg {
+
+// ---------------------------------------------------------------------------
+// Device tables
+
+struct GProblem {  // one problem, as the kernels see it
+  const float* A;
+  const float* B;
+  float* C;
+  long lda, ldb, ldc;
+  int M, N, K, Kp;
+  void* Ap;  // split parts [P][M][Kp]
+  void* Bp;  // split parts [P][N][Kp]
+  uint32_t* rowmax;
+  uint32_t* colmax;
+};
+
+struct GTiles {  // tile source for the tensor-core body
+  const GProblem* probs;
+  const int4* tiles;  // {problem, m0, n0, 0}
+  const CUtensorMap* maps;  // 2 per problem: A parts, B parts
+  int n;
+  __device__ __forceinline__ int count() const { return n; }
+  __device__ __forceinline__ TileWork get(int t) const {
+    const int4 e = tiles[t];
+    const GProblem& p = probs[e.x];
+    TileWork w;
+    w.ma = maps + 2 * e.x;
+    w.mb = maps + 2 * e.x + 1;
+    w.C = p.C;
+    w.ldc = p.ldc;
+    w.M = p.M;
+    w.N = p.N;
+    w.m0 = e.y;
+    w.n0 = e.z;
+    w.KT = p.Kp / kBK;
+    w.rowmax = p.rowmax;
+    w.colmax = p.colmax;
+    return w;
+  }
+};
+
+template <int P, int BN, int STAGES, bool SCALED>
+__global__ void __launch_bounds__(320, 1) tc_grouped_kernel(const GTiles tiles, const TcRun run) {
+  tc_body<P, BN, STAGES, SCALED>(tiles, run);
+}
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
+__global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
+    ffma_grouped_kernel(const GProblem* __restrict__ probs, const int4* __restrict__ tiles, int n) {
+  extern __shared__ __align__(16) float smem[];
+  for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    const int4 e = tiles[t];
+    const GProblem& p = probs[e.x];
+    const bool vec_store = ((p.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
+    __syncthreads();  // the previous tile's last reads of the ring are done
+    ffma_tile<BM, BN, BK, WM, WN, STAGES, VEC, PAIR>(p.A, p.lda, p.B, p.ldb, p.M, p.N, 0, p.K,
+                                                     e.y, e.z, p.C, p.ldc, vec_store, smem);
+  }
+}
+
+// ---- grouped split passes ----------------------------------------------------
+// Jobs are int4 {problem, a, b, c}; one CTA per job.
+
+// A rows: job {problem, first 8-element unit, unit count, 0}; units are
+// row-major over [M][Kp/8].
+template <int P, bool SCALED>
+__global__ void __launch_bounds__(256) gsplit_a_kernel(const GProblem* __restrict__ probs,
+                                                       const int4* __restrict__ jobs) {
+  const int4 j = jobs[blockIdx.x];
+  const GProblem& p = probs[j.x];
+  const int upr = p.Kp / 8;
+  const long plane = (long)p.M * p.Kp;
+  auto* Ap = static_cast<__nv_bfloat16*>(p.Ap);
+  for (int u = threadIdx.x; u < j.z; u += blockDim.x) {
+    const long unit = (long)j.y + u;
+    const int m = (int)(unit / upr);
+    const int k0 = (int)(unit - (long)m * upr) * 8;
+    const int e = SCALED ? exp_from_maxbits(p.rowmax[m]) : 0;
+    const float* src = p.A + (long)m * p.lda + k0;
+    float v[8];
+    if (k0 + 8 <= p.K && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+      const float4 x0 = *reinterpret_cast<const float4*>(src);
+      const float4 x1 = *reinterpret_cast<const float4*>(src + 4);
+      v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
+      v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = (k0 + i < p.K) ? src[i] : 0.0f;
+    }
+    __align__(16) __nv_bfloat16 parts[P][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      __nv_bfloat16 o[3];
+      split_value<P>(v[i], e, o);
+#pragma unroll
+      for (int q = 0; q < P; ++q) parts[q][i] = o[q];
+    }
+    __nv_bfloat16* dst = Ap + (long)m * p.Kp + k0;
+#pragma unroll
+    for (int q = 0; q < P; ++q)
+      *reinterpret_cast<uint4*>(dst + q * plane) = *reinterpret_cast<const uint4*>(parts[q]);
+  }
+}
+
+// B: job {problem, k0, n0, 0}: one 64 x 64 block transposed into [N][Kp].
+template <int P, bool SCALED>
+__global__ void __launch_bounds__(256) gsplit_b_kernel(const GProblem* __restrict__ probs,
+                                                       const int4* __restrict__ jobs) {
+  __shared__ float tile[64][65];
+  const int4 j = jobs[blockIdx.x];
+  const GProblem& p = probs[j.x];
+  split_b_block<P, SCALED>(p.B, p.ldb, p.K, p.N, p.Kp, static_cast<__nv_bfloat16*>(p.Bp),
+                           p.colmax, j.y, j.z, tile);
+}
+
+// Row maxima: job {problem, first row, rows (<= 8), 0}, one warp per row.
+__global__ void __launch_bounds__(256) growmax_kernel(const GProblem* __restrict__ probs,
+                                                      const int4* __restrict__ jobs) {
+  const int4 j = jobs[blockIdx.x];
+  const GProblem& p = probs[j.x];
+  const int w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= j.z) return;
+  const int m = j.y + w;
+  const float* row = p.A + (long)m * p.lda;
+  float mx = 0.0f;
+  for (int k = lane; k < p.K; k += 32) {
+    const float a = fabsf(row[k]);
+    if (isfinite(a)) mx = fmaxf(mx, a);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) p.rowmax[m] = __float_as_uint(mx);
+}
+
+// Column maxima: job {problem, n0, k0, 0}: 256 columns x 256 rows of B.
+__global__ void __launch_bounds__(256) gcolmax_kernel(const GProblem* __restrict__ probs,
+                                                      const int4* __restrict__ jobs) {
+  const int4 j = jobs[blockIdx.x];
+  const GProblem& p = probs[j.x];
+  const int n = j.y + threadIdx.x;
+  if (n >= p.N) return;
+  const int k1 = min(p.K, j.z + 256);
+  float mx = 0.0f;
+  for (int k = j.z; k < k1; ++k) {
+    const float b = fabsf(p.B[(long)k * p.ldb + n]);
+    if (isfinite(b)) mx = fmaxf(mx, b);
+  }
+  if (mx > 0.0f) atomicMax(p.colmax + n, __float_as_uint(mx));
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+
+static size_t al(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+static int parts_of_v(int v) { return (v == HBSG_BF16X6 || v == HBSG_BF16X6_SCALED) ? 3 : 2; }
+static bool scaled_of_v(int v) { return v == HBSG_BF16X3_SCALED || v == HBSG_BF16X6_SCALED; }
+
+struct GLayout {
+  size_t probs_off, tiles_off, maps_off, jobs_off, parts_off, max_off, total;
+  long num_tiles, num_jobs_a, num_jobs_b, num_jobs_rmax, num_jobs_cmax;
+  size_t colmax_bytes;
+};
+
+struct GroupedPlan {
+  int variant;
+  int count;
+  int ffma_tile;  // index into the FFMA table, or -1
+  int tc_tile;    // index into the tensor-core table, or -1
+  GLayout L;
+  uint8_t* ws;
+  int grid;
+  TcRun run;
+  bool vec;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+// Tile counts and job counts for a problem set (host arrays).
+static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, int bm, int bn) {
+  GLayout L{};
+  const bool split = variant != HBSG_FFMA;
+  const int P = split ? parts_of_v(variant) : 0;
+  const bool scaled = split && scaled_of_v(variant);
+  size_t parts = 0, maxes = 0, cmax = 0;
+  for (int i = 0; i < count; ++i) {
+    const hbsg_problem& q = pr[i];
+    if (q.m <= 0 || q.n <= 0) continue;
+    L.num_tiles += (long)((q.m + bm - 1) / bm) * ((q.n + bn - 1) / bn);
+    if (split) {
+      const int Kp = std::max(32, (q.k + 31) / 32 * 32);
+      parts += al((size_t)P * q.m * Kp * 2, 256) + al((size_t)P * q.n * Kp * 2, 256);
+      const long units = (long)q.m * (Kp / 8);
+      L.num_jobs_a += (units + 2047) / 2048;
+      L.num_jobs_b += (long)((Kp + 63) / 64) * ((q.n + 63) / 64);
+      if (scaled) {
+        maxes += al((size_t)q.m * 4, 256);
+        cmax += al((size_t)q.n * 4, 256);
+        L.num_jobs_rmax += (q.m + 7) / 8;
+        L.num_jobs_cmax += (long)((q.n + 255) / 256) * ((q.k + 255) / 256);
+      }
+    }
+  }
+  L.probs_off = 0;
+  L.tiles_off = al(sizeof(GProblem) * (size_t)count, 256);
+  L.maps_off = al(L.tiles_off + sizeof(int4) * (size_t)L.num_tiles, 256);
+  L.jobs_off = al(L.maps_off + (split ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
+  const long jobs = L.num_jobs_a + L.num_jobs_b + L.num_jobs_rmax + L.num_jobs_cmax;
+  L.parts_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);
+  L.max_off = L.parts_off + parts;
+  L.colmax_bytes = cmax;
+  L.total = L.max_off + cmax + maxes;  // colmax block first (one memset), then rowmax
+  return L;
+}
+
+static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* tc_idx, int* bm,
+                       int* bn) {
+  const int nf = ffma_num_tiles();
+  const int tile = cfg && cfg->tile > 0 ? cfg->tile - 1 : -1;
+  hbsg_tile_info info;
+  if (variant == HBSG_FFMA) {
+    int idx = tile >= 0 ? tile : 0;  // default: 128 x 128, packed FMA
+    if (idx >= nf) return false;
+    ffma_tile_info(idx, &info);
+    *ffma_idx = idx;
+    *tc_idx = -1;
+    *bm = info.bm;
+    *bn = info.bn;
+    return true;
+  }
+  const int P = parts_of_v(variant);
+  int idx = -1;
+  if (tile >= 0) {
+    idx = tile - nf;
+    if (idx < 0 || idx >= tc_num_tiles() || tc_tile_parts(idx) != P) return false;
+  } else {
+    for (int i = 0; i < tc_num_tiles(); ++i)  // default: the BN = 256 tile
+      if (tc_tile_parts(i) == P && tc_tile_bn(i) == 256) idx = i;
+  }
+  if (idx < 0) return false;
+  tc_tile_info(idx, &info);
+  *ffma_idx = -1;
+  *tc_idx = idx;
+  *bm = info.bm;
+  *bn = info.bn;
+  return true;
+}
+
+// FFMA grouped instantiations mirror the FFMA tile table (ffma_sgemm.cu).
+struct GFfmaEntry {
+  int smem, threads;
+  const void* kv;
+  const void* ks;
+};
+template <int BM, int BN, int BK, int WM, int WN, int ST, bool PAIR>
+static GFfmaEntry gffma_entry() {
+  using S = FfmaShape<BM, BN, BK, WM, WN, ST>;
+  return {S::kSmemBytes, S::kThreads,
+          reinterpret_cast<const void*>(&ffma_grouped_kernel<BM, BN, BK, WM, WN, ST, true, PAIR>),
+          reinterpret_cast<const void*>(&ffma_grouped_kernel<BM, BN, BK, WM, WN, ST, false, PAIR>)};
+}
+static GFfmaEntry gffma_table(int idx) {
+  switch (idx) {
+    case 0: return gffma_entry<128, 128, 16, 64, 64, 4, true>();
+    case 1: return gffma_entry<128, 256, 16, 64, 64, 4, true>();
+    case 2: return gffma_entry<64, 64, 16, 32, 32, 4, true>();
+    case 3: return gffma_entry<128, 64, 16, 64, 32, 4, true>();
+    case 4: return gffma_entry<128, 256, 32, 64, 64, 3, true>();
+    case 5: return gffma_entry<256, 128, 16, 64, 64, 4, true>();
+    case 6: return gffma_entry<128, 128, 32, 64, 64, 3, true>();
+    case 7: return gffma_entry<128, 128, 16, 64, 64, 4, false>();
+    default: return gffma_entry<128, 256, 16, 64, 64, 4, false>();
+  }
+}
+
+struct GTcEntry {
+  int smem;
+  const void* k0;
+  const void* k1;
+};
+#define HBSG_GTC_ENTRY(P, BN, ST)                                                        \
+  GTcEntry{TcShape<P, BN, ST>::kSmemBytes,                                               \
+           reinterpret_cast<const void*>(&tc_grouped_kernel<P, BN, ST, false>),          \
+           reinterpret_cast<const void*>(&tc_grouped_kernel<P, BN, ST, true>)},
+static const GTcEntry kGTc[] = {HBSG_TC_TILE_LIST(HBSG_GTC_ENTRY)};
+
+static uint32_t g_ffma_masks[9][2];
+static uint32_t g_tc_masks[sizeof(kGTc) / sizeof(kGTc[0])][2];
+
+// Launches of one grouped product on `st` (no host synchronisation, no
+// allocation: capturable).
+static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
+  const GLayout& L = pl.L;
+  const GProblem* probs = reinterpret_cast<const GProblem*>(pl.ws + L.probs_off);
+  const int4* tiles = reinterpret_cast<const int4*>(pl.ws + L.tiles_off);
+  if (L.num_tiles == 0) return cudaSuccess;
+  if (pl.variant == HBSG_FFMA) {
+    const GFfmaEntry e = gffma_table(pl.ffma_tile);
+    const void* k = pl.vec ? e.kv : e.ks;
+    if (!set_smem_once(k, e.smem, &g_ffma_masks[pl.ffma_tile][pl.vec ? 0 : 1]))
+      return cudaErrorInvalidValue;
+    int n = (int)L.num_tiles;
+    void* args[] = {&probs, &tiles, &n};
+    return cudaLaunchKernel(k, dim3(pl.grid), dim3(e.threads), args, e.smem, st);
+  }
+  const int P = parts_of_v(pl.variant);
+  const bool scaled = scaled_of_v(pl.variant);
+  const int4* jobs = reinterpret_cast<const int4*>(pl.ws + L.jobs_off);
+  const int4* ja = jobs;
+  const int4* jb = ja + L.num_jobs_a;
+  const int4* jr = jb + L.num_jobs_b;
+  const int4* jc = jr + L.num_jobs_rmax;
+  if (scaled) {
+    cudaError_t e = cudaMemsetAsync(pl.ws + L.max_off, 0, L.colmax_bytes, st);
+    if (e != cudaSuccess) return e;
+    if (L.num_jobs_rmax) growmax_kernel<<<(unsigned)L.num_jobs_rmax, 256, 0, st>>>(probs, jr);
+    if (L.num_jobs_cmax) gcolmax_kernel<<<(unsigned)L.num_jobs_cmax, 256, 0, st>>>(probs, jc);
+  }
+  if (L.num_jobs_a) {
+    if (P == 3) {
+      if (scaled) gsplit_a_kernel<3, true><<<(unsigned)L.num_jobs_a, 256, 0, st>>>(probs, ja);
+      else gsplit_a_kernel<3, false><<<(unsigned)L.num_jobs_a, 256, 0, st>>>(probs, ja);
+    } else {
+      if (scaled) gsplit_a_kernel<2, true><<<(unsigned)L.num_jobs_a, 256, 0, st>>>(probs, ja);
+      else gsplit_a_kernel<2, false><<<(unsigned)L.num_jobs_a, 256, 0, st>>>(probs, ja);
+    }
+  }
+  if (L.num_jobs_b) {
+    if (P == 3) {
+      if (scaled) gsplit_b_kernel<3, true><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
+      else gsplit_b_kernel<3, false><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
+    } else {
+      if (scaled) gsplit_b_kernel<2, true><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
+      else gsplit_b_kernel<2, false><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const GTcEntry& te = kGTc[pl.tc_tile];
+  const void* k = scaled ? te.k1 : te.k0;
+  if (!set_smem_once(k, te.smem, &g_tc_masks[pl.tc_tile][scaled ? 1 : 0]))
+    return cudaErrorInvalidValue;
+  GTiles gt;
+  gt.probs = probs;
+  gt.tiles = tiles;
+  gt.maps = reinterpret_cast<const CUtensorMap*>(pl.ws + L.maps_off);
+  gt.n = (int)L.num_tiles;
+  TcRun run = pl.run;
+  void* args[] = {&gt, &run};
+  return cudaLaunchKernel(k, dim3(pl.grid), dim3(320), args, te.smem, st);
+}
+
+static int status_of(cudaError_t e) {
+  if (e == cudaSuccess) return HBSG_OK;
+  cudaGetLastError();
+  return (e == cudaErrorInvalidValue || e == cudaErrorLaunchOutOfResources) ? HBSG_ERR_LAUNCH
+                                                                            : HBSG_ERR_CUDA;
+}
+
+static int validate(int count, const hbsg_problem* pr, int variant) {
+  if (count < 0 || (count > 0 && !pr)) return HBSG_ERR_INVALID_ARG;
+  if (variant < HBSG_FFMA || variant > HBSG_BF16X6_SCALED) return HBSG_ERR_UNSUPPORTED;
+  for (int i = 0; i < count; ++i) {
+    const hbsg_problem& q = pr[i];
+    if (q.m < 0 || q.n < 0 || q.k < 0) return HBSG_ERR_INVALID_ARG;
+    if (q.m == 0 || q.n == 0) continue;
+    if (!q.c || q.ldc < q.n) return HBSG_ERR_INVALID_ARG;
+    if (q.k > 0 && (!q.a || !q.b || q.lda < q.k || q.ldb < q.n)) return HBSG_ERR_INVALID_ARG;
+    if ((long)q.m * ((q.k + 31) / 32 * 4) > 0x7fffffffL) return HBSG_ERR_UNSUPPORTED;
+  }
+  return HBSG_OK;
+}
+
+// Builds the host copies of the tables and uploads them into the workspace.
+static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const hbsg_config* cfg,
+                      void* ws, size_t ws_bytes) {
+  int bm = 0, bn = 0;
+  if (!tile_shape(pl->variant, cfg, &pl->ffma_tile, &pl->tc_tile, &bm, &bn))
+    return HBSG_ERR_UNSUPPORTED;
+  pl->count = count;
+  pl->L = grouped_layout(count, pr, pl->variant, bm, bn);
+  const GLayout& L = pl->L;
+  if (!ws || ws_bytes < L.total || (reinterpret_cast<uintptr_t>(ws) & 255)) return HBSG_ERR_WORKSPACE;
+  pl->ws = static_cast<uint8_t*>(ws);
+  const int sms = current_device_sms(nullptr);
+  if (sms < 0) return HBSG_ERR_NO_DEVICE;
+  const bool split = pl->variant != HBSG_FFMA;
+  const int P = split ? parts_of_v(pl->variant) : 0;
+  const bool scaled = split && scaled_of_v(pl->variant);
+
+  std::vector<GProblem> probs(count);
+  size_t parts_cur = L.parts_off, cmax_cur = L.max_off, rmax_cur = L.max_off + L.colmax_bytes;
+  pl->vec = true;
+  for (int i = 0; i < count; ++i) {
+    const hbsg_problem& q = pr[i];
+    GProblem g{};
+    g.A = q.a;
+    g.B = q.b;
+    g.C = q.c;
+    g.lda = q.lda;
+    g.ldb = q.ldb;
+    g.ldc = q.ldc;
+    g.M = q.m;
+    g.N = q.n;
+    g.K = q.k;
+    g.Kp = std::max(32, (q.k + 31) / 32 * 32);
+    if (q.m > 0 && q.n > 0) {
+      if ((q.lda & 3) || (q.ldb & 3) || (reinterpret_cast<uintptr_t>(q.a) & 15) ||
+          (reinterpret_cast<uintptr_t>(q.b) & 15))
+        pl->vec = false;
+      if (split) {
+        g.Ap = pl->ws + parts_cur;
+        parts_cur += al((size_t)P * q.m * g.Kp * 2, 256);
+        g.Bp = pl->ws + parts_cur;
+        parts_cur += al((size_t)P * q.n * g.Kp * 2, 256);
+        if (scaled) {
+          g.colmax = reinterpret_cast<uint32_t*>(pl->ws + cmax_cur);
+          cmax_cur += al((size_t)q.n * 4, 256);
+          g.rowmax = reinterpret_cast<uint32_t*>(pl->ws + rmax_cur);
+          rmax_cur += al((size_t)q.m * 4, 256);
+        }
+      }
+    }
+    probs[i] = g;
+  }
+
+  // tile list: problems by K descending (stable), rasterised tiles inside
+  std::vector<int> order(count);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return pr[x].k > pr[y].k; });
+  const int raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 8;
+  std::vector<int4> tiles;
+  tiles.reserve(L.num_tiles);
+  for (int i : order) {
+    const hbsg_problem& q = pr[i];
+    if (q.m <= 0 || q.n <= 0) continue;
+    const int tm = (q.m + bm - 1) / bm, tn = (q.n + bn - 1) / bn;
+    for (int g0 = 0; g0 < tm; g0 += raster) {
+      const int gm = std::min(raster, tm - g0);
+      for (int c = 0; c < tn; ++c)
+        for (int r = 0; r < gm; ++r) tiles.push_back(make_int4(i, (g0 + r) * bm, c * bn, 0));
+    }
+  }
+
+  std::vector<int4> jobs;
+  std::vector<CUtensorMap> maps;
+  if (split) {
+    for (int i = 0; i < count; ++i) {  // A split jobs
+      const GProblem& g = probs[i];
+      if (g.M <= 0 || g.N <= 0) continue;
+      const long units = (long)g.M * (g.Kp / 8);
+      for (long u = 0; u < units; u += 2048)
+        jobs.push_back(make_int4(i, (int)u, (int)std::min<long>(2048, units - u), 0));
+    }
+    for (int i = 0; i < count; ++i) {  // B split jobs
+      const GProblem& g = probs[i];
+      if (g.M <= 0 || g.N <= 0) continue;
+      for (int k0 = 0; k0 < g.Kp; k0 += 64)
+        for (int n0 = 0; n0 < g.N; n0 += 64) jobs.push_back(make_int4(i, k0, n0, 0));
+    }
+    if (scaled) {
+      for (int i = 0; i < count; ++i) {
+        const GProblem& g = probs[i];
+        if (g.M <= 0 || g.N <= 0) continue;
+        for (int m0 = 0; m0 < g.M; m0 += 8) jobs.push_back(make_int4(i, m0, std::min(8, g.M - m0), 0));
+      }
+      for (int i = 0; i < count; ++i) {
+        const GProblem& g = probs[i];
+        if (g.M <= 0 || g.N <= 0) continue;
+        for (int n0 = 0; n0 < g.N; n0 += 256)
+          for (int k0 = 0; k0 < g.K; k0 += 256) jobs.push_back(make_int4(i, n0, k0, 0));
+      }
+    }
+    maps.resize(2 * (size_t)count);
+    for (int i = 0; i < count; ++i) {
+      const GProblem& g = probs[i];
+      if (g.M <= 0 || g.N <= 0) {
+        memset(&maps[2 * i], 0, 2 * sizeof(CUtensorMap));
+        continue;
+      }
+      if (!tc_make_parts_map(&maps[2 * i], g.Ap, P, g.M, g.Kp, kBM) ||
+          !tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp, bn))
+        return HBSG_ERR_UNSUPPORTED;
+    }
+    pl->run.chunk_ktiles = tc_chunk_ktiles(P, cfg ? cfg->chunk_k : 0);
+    pl->run.wait_limit_ns = kWaitLimitNs;
+    pl->run.debug_skip_loads = 0;
+  }
+
+  // one synchronous upload per table
+  cudaError_t e = cudaMemcpy(pl->ws + L.probs_off, probs.data(), sizeof(GProblem) * count,
+                             cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMemcpy(pl->ws + L.tiles_off, tiles.data(), sizeof(int4) * tiles.size(),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !maps.empty())
+    e = cudaMemcpy(pl->ws + L.maps_off, maps.data(), sizeof(CUtensorMap) * maps.size(),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !jobs.empty())
+    e = cudaMemcpy(pl->ws + L.jobs_off, jobs.data(), sizeof(int4) * jobs.size(),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return status_of(e);
+
+  const long slots = split ? sms : (long)sms * (gffma_table(pl->ffma_tile).threads <= 128 ? 2 : 1);
+  pl->grid = (int)std::max<long>(1, std::min<long>(slots, L.num_tiles));
+  return HBSG_OK;
+}
+
+int grouped_read_and_clear_device_error() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int)) != cudaSuccess) return HBSG_ERR_CUDA;
+  if (v != 0) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int));
+  }
+  return v;
+}
+
+}  // namespace hbsg
+
+using namespace hbsg;
+
+struct hbsg_grouped_plan_s {
+  GroupedPlan p;
+};
+
+extern "C" {
+
+size_t hbsg_grouped_workspace_size(int count, const hbsg_problem* problems, int variant,
+                                   const hbsg_config* cfg) {
+  if (validate(count, problems, variant) != HBSG_OK) return 0;
+  int fi, ti, bm, bn;
+  if (!tile_shape(variant, cfg, &fi, &ti, &bm, &bn)) return 0;
+  return grouped_layout(count, problems, variant, bm, bn).total;
+}
+
+int hbsg_grouped_plan_create(hbsg_grouped_plan* out, int count, const hbsg_problem* problems,
+                             int variant, const hbsg_config* cfg, void* workspace,
+                             size_t workspace_bytes) {
+  if (!out) return HBSG_ERR_INVALID_ARG;
+  *out = nullptr;
+  int st = validate(count, problems, variant);
+  if (st != HBSG_OK) return st;
+  auto* h = new (std::nothrow) hbsg_grouped_plan_s();
+  if (!h) return HBSG_ERR_INVALID_ARG;
+  h->p.variant = variant;
+  st = plan_build(&h->p, count, problems, cfg, workspace, workspace_bytes);
+  if (st != HBSG_OK) {
+    delete h;
+    return st;
+  }
+  // Capture the launches once on a private stream; runs replay the graph.
+  cudaStream_t cs = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const cudaError_t le = grouped_launch(h->p, cs);
+    e = cudaStreamEndCapture(cs, &h->p.graph);
+    if (le != cudaSuccess) e = le;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->p.exec, h->p.graph, 0);
+  if (cs) cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    if (h->p.exec) cudaGraphExecDestroy(h->p.exec);
+    if (h->p.graph) cudaGraphDestroy(h->p.graph);
+    delete h;
+    return status_of(e);
+  }
+  *out = h;
+  return HBSG_OK;
+}
+
+int hbsg_grouped_run(hbsg_grouped_plan plan, hbsg_stream_t stream) {
+  if (!plan || !plan->p.exec) return HBSG_ERR_INVALID_ARG;
+  return status_of(cudaGraphLaunch(plan->p.exec, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int hbsg_grouped_plan_destroy(hbsg_grouped_plan plan) {
+  if (!plan) return HBSG_ERR_INVALID_ARG;
+  if (plan->p.exec) cudaGraphExecDestroy(plan->p.exec);
+  if (plan->p.graph) cudaGraphDestroy(plan->p.graph);
+  delete plan;
+  return HBSG_OK;
+}
+
+int hbsg_gemm_grouped(int count, const hbsg_problem* problems, int variant, const hbsg_config* cfg,
+                      void* workspace, size_t workspace_bytes, hbsg_stream_t stream) {
+  int st = validate(count, problems, variant);
+  if (st != HBSG_OK) return st;
+  GroupedPlan p{};
+  p.variant = variant;
+  // The tables are uploaded with blocking copies; order them after prior
+  // work on `stream` that may still read the workspace.
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return status_of(cudaGetLastError());
+  st = plan_build(&p, count, problems, cfg, workspace, workspace_bytes);
+  if (st != HBSG_OK) return st;
+  return status_of(grouped_launch(p, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+}  // extern "C"

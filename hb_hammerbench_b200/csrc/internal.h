@@ -44,7 +44,11 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
                       float* C, long ldc, const uint32_t* rowmax, const uint32_t* colmax,
                       int raster, int chunk_k, int sms, int debug_skip_loads,
                       unsigned long long wait_limit_ns, cudaStream_t st);
-int read_and_clear_device_error();
+int tc_read_and_clear_device_error();
+int grouped_read_and_clear_device_error();
+int tc_chunk_ktiles(int parts, int chunk_k);
+bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, int box_rows);
+int tc_tile_bn(int idx);
 
 // ---- device state -------------------------------------------------------------
 // Returns the SM count of the current device (cached per device), or -1 when

@@ -14,34 +14,10 @@
 // FP32 bit patterns (non-negative floats order like their bit patterns, so an
 // integer atomicMax is an exact, order-independent max), then derive
 // e = frexp exponent of that max: the row's largest |x'| lies in [0.5, 1).
-#include <cuda_bf16.h>
-
-#include "common.cuh"
 #include "internal.h"
+#include "split_kernel.cuh"
 
 namespace hbsg {
-
-HBSG_DEV int exp_from_maxbits(uint32_t bits) {
-  const float mx = __uint_as_float(bits);
-  if (!(mx > 0.0f) || !isfinite(mx)) return 0;
-  int e;
-  frexpf(mx, &e);
-  return e;
-}
-
-template <int P>
-HBSG_DEV void split_value(float x, int e, __nv_bfloat16* out) {
-  if (e != 0) x = ldexpf(x, -e);
-  const __nv_bfloat16 h = __float2bfloat16_rn(x);
-  const float r1 = x - __bfloat162float(h);
-  const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-  out[0] = h;
-  out[1] = m;
-  if constexpr (P == 3) {
-    const float r2 = r1 - __bfloat162float(m);
-    out[2] = __float2bfloat16_rn(r2);
-  }
-}
 
 // max|A[m][k]| over k per row, one warp per row.
 __global__ void row_maxabs_kernel(const float* __restrict__ A, long lda, int M, int K,
@@ -113,48 +89,13 @@ __global__ void split_a_kernel(const float* __restrict__ A, long lda, int M, int
   }
 }
 
-// B (K x N, row stride ldb) -> Bp[p][n][0..Kp) through a 64 x 64 shared tile.
+// B (K x N, row stride ldb) -> Bp[p][n][0..Kp) through 64 x 64 shared tiles.
 template <int P, bool SCALED>
 __global__ void __launch_bounds__(256) split_b_kernel(const float* __restrict__ B, long ldb, int K,
                                                       int N, int Kp, __nv_bfloat16* __restrict__ Bp,
                                                       const uint32_t* __restrict__ colmax) {
   __shared__ float tile[64][65];
-  const int k0 = blockIdx.y * 64;
-  const int n0 = blockIdx.x * 64;
-  const int tid = threadIdx.x;
-  // load: 64 rows (k) x 64 columns (n), coalesced along n
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const int idx = tid + i * 256;
-    const int r = idx >> 6;
-    const int c = idx & 63;
-    const int k = k0 + r;
-    const int n = n0 + c;
-    tile[r][c] = (k < K && n < N) ? B[(long)k * ldb + n] : 0.0f;
-  }
-  __syncthreads();
-  const long plane = (long)N * Kp;
-  // store: 8 threads per output row n, each 8 consecutive k
-#pragma unroll
-  for (int pass = 0; pass < 2; ++pass) {
-    const int j = pass * 32 + (tid >> 3);  // n offset
-    const int kk = (tid & 7) * 8;          // k offset
-    const int n = n0 + j;
-    if (n >= N || k0 + kk >= Kp) continue;
-    const int e = SCALED ? exp_from_maxbits(colmax[n]) : 0;
-    __align__(16) __nv_bfloat16 parts[P][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      __nv_bfloat16 o[3];
-      split_value<P>(tile[kk + i][j], e, o);
-#pragma unroll
-      for (int p = 0; p < P; ++p) parts[p][i] = o[p];
-    }
-    __nv_bfloat16* dst = Bp + (long)n * Kp + k0 + kk;
-#pragma unroll
-    for (int p = 0; p < P; ++p)
-      *reinterpret_cast<uint4*>(dst + p * plane) = *reinterpret_cast<const uint4*>(parts[p]);
-  }
+  split_b_block<P, SCALED>(B, ldb, K, N, Kp, Bp, colmax, blockIdx.y * 64, blockIdx.x * 64, tile);
 }
 
 static int grid_for(long work, int per_block, int sms) {

@@ -25,371 +25,65 @@
 // No TMA multicast is used; every CTA fetches its own tiles.
 // Every wait is bounded: after kWaitLimitNs the kernel records
 // HBSG_ERR_DEVICE_TIMEOUT in the device error flag and unwinds.
-#include <cuda.h>
-#include <cuda_bf16.h>
-#include <cudaTypedefs.h>
-
-#include "common.cuh"
-#include "internal.h"
+#include "tc_kernel.cuh"
 
 namespace hbsg {
-
-__device__ int g_device_error = 0;
-
-static constexpr int kBM = 128;
-static constexpr int kBK = 32;  // bf16 elements per k-tile row = 64 bytes = one swizzle row
-static constexpr unsigned long long kWaitLimitNs = 4000000000ull;  // default bound: 4 s
 
 struct TcParams {
   int M, N, K, Kp;
   int tiles_m, tiles_n, num_tiles;
   int raster;
-  int chunk_ktiles;  // k-tiles accumulated in TMEM before draining
   float* C;
   long ldc;
   const uint32_t* rowmax;  // null unless scaled
   const uint32_t* colmax;
-  unsigned long long wait_limit_ns;  // bound of every mbarrier wait
-  int debug_skip_loads;    // test hook: producer never loads (forces the timeout path)
 };
 
-HBSG_DEV unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait on an mbarrier phase. Returns false (and raises the flags) on
-// timeout or when another role already aborted.
-HBSG_DEV bool wait_bounded(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                          unsigned long long limit_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer();
-  for (uint32_t i = 0;; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 63) == 0) {
-      if (*abort_flag) return false;
-      if (globaltimer() - t0 > limit_ns) {
-        *abort_flag = 1;
-        atomicExch(&g_device_error, (int)HBSG_ERR_DEVICE_TIMEOUT);
-        return false;
-      }
-    }
-  }
-}
-
-HBSG_DEV void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
-                          uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-
-HBSG_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
-HBSG_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
-
-HBSG_DEV void tc_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-
-HBSG_DEV void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                     uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-// 32 lanes x 32 columns of 32-bit TMEM into 32 registers per thread.
-HBSG_DEV void tmem_ld32(uint32_t taddr, float* v) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// Shared-memory matrix descriptor: K-major, 64-byte swizzle, rows of 64 bytes,
-// 8-row core groups 512 bytes apart (SBO), LBO unused for swizzled K-major
-// (encoded 1), descriptor version 1 (bits 46-47), layout type 4 = SWIZZLE_64B.
-HBSG_DEV uint64_t sw64_desc(uint32_t saddr) {
-  return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
-}
-
-// Instruction descriptor, kind::f16: D f32 (bits 4-5 = 1), A and B bf16
-// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
-__host__ __device__ constexpr uint32_t f16_idesc(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-// Product q of the P-part form as (A part, B part), smallest term first.
-// P = 2: (hi,mid) (mid,hi) (hi,hi)
-// P = 3: (mid,mid) (hi,lo) (lo,hi) (hi,mid) (mid,hi) (hi,hi)
-template <int P>
-struct Products {
-  static constexpr int n = P == 3 ? 6 : 3;
-  __host__ __device__ static constexpr int a(int q) {
-    return P == 3 ? (q == 0 ? 1 : q == 2 ? 2 : q == 4 ? 1 : 0) : (q == 1 ? 1 : 0);
-  }
-  __host__ __device__ static constexpr int b(int q) {
-    return P == 3 ? (q == 0 ? 1 : q == 1 ? 2 : q == 3 ? 1 : 0) : (q == 0 ? 1 : 0);
+// Tiles of one GEMM in rasterised order: groups of `raster` tile rows,
+// column-major inside a group, so CTAs resident together share operand
+// strips in L2.
+struct SingleTiles {
+  const CUtensorMap* ma;
+  const CUtensorMap* mb;
+  const TcParams* p;
+  template <int BN>
+  __device__ __forceinline__ TileWork get_bn(int t) const {
+    const int span = p->raster * p->tiles_n;
+    const int g = t / span;
+    const int first = g * p->raster;
+    const int gm = min(p->raster, p->tiles_m - first);
+    const int in = t - g * span;
+    TileWork w;
+    w.ma = ma;
+    w.mb = mb;
+    w.C = p->C;
+    w.ldc = p->ldc;
+    w.M = p->M;
+    w.N = p->N;
+    w.m0 = (first + in % gm) * kBM;
+    w.n0 = (in / gm) * BN;
+    w.KT = p->Kp / kBK;
+    w.rowmax = p->rowmax;
+    w.colmax = p->colmax;
+    return w;
   }
 };
-static_assert(Products<3>::a(0) == 1 && Products<3>::b(0) == 1, "mid*mid");
-static_assert(Products<3>::a(1) == 0 && Products<3>::b(1) == 2, "hi*lo");
-static_assert(Products<3>::a(2) == 2 && Products<3>::b(2) == 0, "lo*hi");
-static_assert(Products<3>::a(3) == 0 && Products<3>::b(3) == 1, "hi*mid");
-static_assert(Products<3>::a(4) == 1 && Products<3>::b(4) == 0, "mid*hi");
-static_assert(Products<3>::a(5) == 0 && Products<3>::b(5) == 0, "hi*hi");
-static_assert(Products<2>::a(0) == 0 && Products<2>::b(0) == 1, "hi*mid");
-static_assert(Products<2>::a(1) == 1 && Products<2>::b(1) == 0, "mid*hi");
-static_assert(Products<2>::a(2) == 0 && Products<2>::b(2) == 0, "hi*hi");
 
-template <int P, int BN, int STAGES>
-struct TcShape {
-  static constexpr int kABytes = kBM * kBK * 2;  // one part
-  static constexpr int kBBytes = BN * kBK * 2;
-  static constexpr int kStageBytes = P * (kABytes + kBBytes);
-  static constexpr int kTmemCols = 2 * BN;  // two accumulator buffers
-  static constexpr int kAllocCols = kTmemCols <= 32 ? 32 : kTmemCols <= 64 ? 64 : kTmemCols <= 128 ? 128 : kTmemCols <= 256 ? 256 : 512;
-  static constexpr int kBarBytes = 8 * (2 * STAGES + 4) + 16;
-  static constexpr int kSmemBytes = 1024 + STAGES * kStageBytes + kBarBytes;
-  static constexpr int kThreads = 320;
-  static_assert(kSmemBytes <= 232448, "shared memory");
-  static_assert(BN % 16 == 0 && BN >= 64 && BN <= 256, "UMMA N");
+template <int BN>
+struct SingleTilesBN : SingleTiles {
+  __device__ __forceinline__ int count() const { return p->num_tiles; }
+  __device__ __forceinline__ TileWork get(int t) const { return get_bn<BN>(t); }
 };
 
 template <int P, int BN, int STAGES, bool SCALED>
 __global__ void __launch_bounds__(320, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                   TcParams p) {
-  using S = TcShape<P, BN, STAGES>;
-  extern __shared__ uint8_t smem_raw[];
-  const uint32_t raw = smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;
-  uint8_t* smem = smem_raw + (base - raw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * S::kStageBytes);
-  uint64_t* full = bars;
-  uint64_t* empty = bars + STAGES;
-  uint64_t* tfull = bars + 2 * STAGES;
-  uint64_t* tempty = bars + 2 * STAGES + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
-    }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 8);
-    }
-    *abort_flag = 0;
-    fence_barrier_init();
-  }
-  if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                     smem_u32(tmem_slot)),
-                 "r"(S::kAllocCols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
-  }
-  if (warp == 0 && lane == 0) {
-    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
-    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem_base = *tmem_slot;
-
-  const int KT = p.Kp / kBK;
-  const int nchunks = (KT + p.chunk_ktiles - 1) / p.chunk_ktiles;
-
-  auto tile_coords = [&](int t, int& m0, int& n0) {
-    const int span = p.raster * p.tiles_n;
-    const int g = t / span;
-    const int first = g * p.raster;
-    const int gm = min(p.raster, p.tiles_m - first);
-    const int in = t - g * span;
-    m0 = (first + in % gm) * kBM;
-    n0 = (in / gm) * BN;
-  };
-
-  if (warp == 0) {
-    // ---------------- TMA producer ----------------
-    if (lane == 0) {
-      uint32_t it = 0;
-      bool ok = true;
-      for (int t = blockIdx.x; t < p.num_tiles && ok; t += gridDim.x) {
-        int m0, n0;
-        tile_coords(t, m0, n0);
-        for (int kt = 0; kt < KT; ++kt, ++it) {
-          const int s = it % STAGES;
-          const uint32_t ph = (it / STAGES) & 1;
-          if (!wait_bounded(&empty[s], ph ^ 1, abort_flag, p.wait_limit_ns)) {
-            ok = false;
-            break;
-          }
-          if (p.debug_skip_loads) continue;
-          const uint32_t sa = base + s * S::kStageBytes;
-          const uint32_t sb = sa + P * S::kABytes;
-          mbar_arrive_expect_tx(&full[s], S::kStageBytes);
-          tma_load_3d(sa, &tmA, kt * kBK, m0, 0, &full[s]);
-          tma_load_3d(sb, &tmB, kt * kBK, n0, 0, &full[s]);
-        }
-      }
-    }
-  } else if (warp == 1) {
-    // ---------------- MMA issuer ----------------
-    if (lane == 0) {
-      constexpr uint32_t idesc = f16_idesc(kBM, BN);
-      uint32_t it = 0, ch = 0;
-      bool ok = true;
-      for (int t = blockIdx.x; t < p.num_tiles && ok; t += gridDim.x) {
-        int kt = 0;
-        for (int c = 0; c < nchunks && ok; ++c, ++ch) {
-          const int buf = ch & 1;
-          if (!wait_bounded(&tempty[buf], ((ch >> 1) & 1) ^ 1, abort_flag, p.wait_limit_ns)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint32_t d = tmem_base + buf * BN;
-          const int kend = min(KT, kt + p.chunk_ktiles);
-          bool first = true;
-          for (; kt < kend; ++kt, ++it) {
-            const int s = it % STAGES;
-            if (!wait_bounded(&full[s], (it / STAGES) & 1, abort_flag, p.wait_limit_ns)) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t sa = base + s * S::kStageBytes;
-            const uint32_t sb = sa + P * S::kABytes;
-#pragma unroll
-            for (int ks = 0; ks < kBK / 16; ++ks) {
-#pragma unroll
-              for (int q = 0; q < Products<P>::n; ++q) {
-                const uint64_t ad = sw64_desc(sa + Products<P>::a(q) * S::kABytes + ks * 32);
-                const uint64_t bd = sw64_desc(sb + Products<P>::b(q) * S::kBBytes + ks * 32);
-                tc_mma(d, ad, bd, idesc, first ? 0u : 1u);
-                first = false;
-              }
-            }
-            tc_commit(&empty[s]);
-          }
-          if (ok) tc_commit(&tfull[buf]);
-        }
-      }
-    }
-  } else {
-    // ---------------- epilogue (warps 2..9) ----------------
-    const int q = warp & 3;            // TMEM lane quadrant this warp may access
-    const int h = (warp - 2) >> 2;     // column half
-    constexpr int COLS = BN / 2;
-    uint32_t ch = 0;
-    bool ok = true;
-    for (int t = blockIdx.x; t < p.num_tiles && ok; t += gridDim.x) {
-      int m0, n0;
-      tile_coords(t, m0, n0);
-      float sum[COLS];
-#pragma unroll
-      for (int i = 0; i < COLS; ++i) sum[i] = 0.0f;
-      for (int c = 0; c < nchunks; ++c, ++ch) {
-        const int buf = ch & 1;
-        int got = 0;
-        if (lane == 0) got = wait_bounded(&tfull[buf], (ch >> 1) & 1, abort_flag, p.wait_limit_ns);
-        got = __shfl_sync(0xffffffffu, got, 0);
-        if (!got) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + buf * BN + h * COLS;
-#pragma unroll
-        for (int j = 0; j < COLS / 32; ++j) {
-          float v[32];
-          tmem_ld32(taddr + 32 * j, v);
-#pragma unroll
-          for (int i = 0; i < 32; ++i) sum[32 * j + i] += v[i];
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[buf]);
-      }
-      if (!ok) break;
-      const int row = m0 + 32 * q + lane;
-      const int col0 = n0 + h * COLS;
-      if (row < p.M) {
-        float* crow = p.C + (long)row * p.ldc;
-        int er = 0;
-        if constexpr (SCALED) {
-          const float mx = __uint_as_float(p.rowmax[row]);
-          if (mx > 0.0f && isfinite(mx)) frexpf(mx, &er);
-        }
-        const bool vec = ((p.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
-#pragma unroll
-        for (int j = 0; j < COLS; j += 4) {
-          float o[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            float x = sum[j + e];
-            if constexpr (SCALED) {
-              const int cc = min(col0 + j + e, p.N - 1);
-              const float mx = __uint_as_float(p.colmax[cc]);
-              int ec = 0;
-              if (mx > 0.0f && isfinite(mx)) frexpf(mx, &ec);
-              x = ldexpf(x, er + ec);
-            }
-            o[e] = x;
-          }
-          const int c = col0 + j;
-          if (vec && c + 3 < p.N) {
-            *reinterpret_cast<float4*>(crow + c) = make_float4(o[0], o[1], o[2], o[3]);
-          } else {
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-              if (c + e < p.N) crow[c + e] = o[e];
-          }
-        }
-      }
-    }
-  }
-
-  // All roles leave their loops (normally or through a bounded abort); MMAs
-  // the epilogue waited for are complete. On abort, give in-flight tensor-core
-  // work a bounded moment before the TMEM is released.
-  __syncthreads();
-  if (*abort_flag) {
-    const unsigned long long t0 = globaltimer();
-    while (globaltimer() - t0 < 2000000ull) {
-    }
-  }
-  if (warp == 1) {
-    __syncwarp();
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base),
-                 "r"(S::kAllocCols));
-  }
+                   const __grid_constant__ TcParams p, const TcRun run) {
+  SingleTilesBN<BN> tiles;
+  tiles.ma = &tmA;
+  tiles.mb = &tmB;
+  tiles.p = &p;
+  tc_body<P, BN, STAGES, SCALED>(tiles, run);
 }
 
 // ---------------------------------------------------------------------------
@@ -411,7 +105,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 // 3-D map over parts[P][rows][Kp] bf16 with a box of {32, box_rows, P}.
-static bool make_parts_map(CUtensorMap* map, const void* parts, int P, int rows, int Kp,
+bool tc_make_parts_map_impl(CUtensorMap* map, const void* parts, int P, int rows, int Kp,
                            int box_rows) {
   auto enc = get_encode();
   if (!enc) return false;
@@ -428,13 +122,13 @@ static bool make_parts_map(CUtensorMap* map, const void* parts, int P, int rows,
 struct TcEntry {
   int parts, bn, stages;
   int smem;
-  cudaError_t (*launch)(const CUtensorMap&, const CUtensorMap&, const TcParams&, int grid,
-                        cudaStream_t, bool scaled);
+  cudaError_t (*launch)(const CUtensorMap&, const CUtensorMap&, const TcParams&, const TcRun&,
+                        int grid, cudaStream_t, bool scaled);
 };
 
 template <int P, int BN, int STAGES>
 static cudaError_t launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p,
-                             int grid, cudaStream_t st, bool scaled) {
+                             const TcRun& run, int grid, cudaStream_t st, bool scaled) {
   using S = TcShape<P, BN, STAGES>;
   auto k0 = tc_gemm_kernel<P, BN, STAGES, false>;
   auto k1 = tc_gemm_kernel<P, BN, STAGES, true>;
@@ -442,7 +136,7 @@ static cudaError_t launch_tc(const CUtensorMap& a, const CUtensorMap& b, const T
   static uint32_t m0 = 0, m1 = 0;
   if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, scaled ? &m1 : &m0))
     return cudaErrorInvalidValue;
-  k<<<grid, S::kThreads, S::kSmemBytes, st>>>(a, b, p);
+  k<<<grid, S::kThreads, S::kSmemBytes, st>>>(a, b, p, run);
   return cudaGetLastError();
 }
 
@@ -450,14 +144,8 @@ static cudaError_t launch_tc(const CUtensorMap& a, const CUtensorMap& b, const T
   TcEntry { P, BN, ST, TcShape<P, BN, ST>::kSmemBytes, &launch_tc<P, BN, ST> }
 
 // Ordered by parts: entries with parts == 3 serve BF16X6, parts == 2 BF16X3.
-static const TcEntry kTcTiles[] = {
-    HBSG_TC_ENTRY(3, 256, 3),  // 128 x 256, 6 products
-    HBSG_TC_ENTRY(3, 128, 4),  // 128 x 128
-    HBSG_TC_ENTRY(3, 64, 6),   // 128 x 64, narrow N
-    HBSG_TC_ENTRY(2, 256, 4),  // 128 x 256, 3 products
-    HBSG_TC_ENTRY(2, 128, 6),  // 128 x 128
-    HBSG_TC_ENTRY(2, 64, 8),   // 128 x 64
-};
+#define HBSG_TC_ENTRY_COMMA(P, BN, ST) HBSG_TC_ENTRY(P, BN, ST),
+static const TcEntry kTcTiles[] = {HBSG_TC_TILE_LIST(HBSG_TC_ENTRY_COMMA)};
 static constexpr int kNumTcTiles = sizeof(kTcTiles) / sizeof(kTcTiles[0]);
 
 int tc_num_tiles() { return kNumTcTiles; }
@@ -475,6 +163,11 @@ bool tc_tile_info(int idx, hbsg_tile_info* out) {
 }
 
 int tc_tile_parts(int idx) { return kTcTiles[idx].parts; }
+int tc_tile_bn(int idx) { return kTcTiles[idx].bn; }
+
+bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, int box_rows) {
+  return tc_make_parts_map_impl(static_cast<CUtensorMap*>(map), parts, P, rows, Kp, box_rows);
+}
 
 int tc_pick_tile(int M, int N, int parts, int sms) {
   int best = -1;
@@ -502,8 +195,8 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
                       unsigned long long wait_limit_ns, cudaStream_t st) {
   const TcEntry& e = kTcTiles[idx];
   CUtensorMap ma, mb;
-  if (!make_parts_map(&ma, Ap, e.parts, M, Kp, kBM)) return cudaErrorInvalidValue;
-  if (!make_parts_map(&mb, Bp, e.parts, N, Kp, e.bn)) return cudaErrorInvalidValue;
+  if (!tc_make_parts_map_impl(&ma, Ap, e.parts, M, Kp, kBM)) return cudaErrorInvalidValue;
+  if (!tc_make_parts_map_impl(&mb, Bp, e.parts, N, Kp, e.bn)) return cudaErrorInvalidValue;
   TcParams p{};
   p.M = M;
   p.N = N;
@@ -513,22 +206,27 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
   p.tiles_n = (N + e.bn - 1) / e.bn;
   p.num_tiles = p.tiles_m * p.tiles_n;
   p.raster = raster > 0 ? raster : 16;
-  // Default drain interval: every k-tile for the 6-product form (its error is
-  // dominated by tensor-core accumulation, and draining is free at this rate),
-  // every 4 k-tiles for the 3-product form (dominated by the 2-part split).
-  int ck = chunk_k > 0 ? chunk_k : (e.parts == 3 ? 32 : 128);
-  p.chunk_ktiles = ck / kBK > 0 ? ck / kBK : 1;
   p.C = C;
   p.ldc = ldc;
   p.rowmax = rowmax;
   p.colmax = colmax;
-  p.debug_skip_loads = debug_skip_loads;
-  p.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;
+  TcRun run;
+  run.chunk_ktiles = tc_chunk_ktiles(e.parts, chunk_k);
+  run.debug_skip_loads = debug_skip_loads;
+  run.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;
   const int grid = p.num_tiles < sms ? p.num_tiles : sms;
-  return e.launch(ma, mb, p, grid, st, rowmax != nullptr);
+  return e.launch(ma, mb, p, run, grid, st, rowmax != nullptr);
 }
 
-int read_and_clear_device_error() {
+// Default drain interval: every k-tile for the 6-product form (its error is
+// dominated by tensor-core accumulation, and draining is free at this rate),
+// every 4 k-tiles for the 3-product form (dominated by the 2-part split).
+int tc_chunk_ktiles(int parts, int chunk_k) {
+  const int ck = chunk_k > 0 ? chunk_k : (parts == 3 ? 32 : 128);
+  return ck / kBK > 0 ? ck / kBK : 1;
+}
+
+int tc_read_and_clear_device_error() {
   int v = 0;
   if (cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int)) != cudaSuccess) return HBSG_ERR_CUDA;
   if (v != 0) {

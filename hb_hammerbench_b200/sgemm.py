@@ -126,6 +126,81 @@ def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, varian
     return c
 
 
+def _problems(As, Bs, Cs):
+    arr = (_lib.Problem * len(As))()
+    for i, (a, b, c) in enumerate(zip(As, Bs, Cs)):
+        for name, t in (("a", a), ("b", b), ("c", c)):
+            _check_f32_cuda(name, t)
+            if t.dim() != 2 or (t.numel() and t.stride(1) != 1):
+                raise ValueError(f"problem {i}: {name} must be 2-D with unit inner stride")
+        m, k = a.shape
+        k2, n = b.shape
+        if k != k2 or tuple(c.shape) != (m, n):
+            raise ValueError(f"problem {i}: shapes {tuple(a.shape)} x {tuple(b.shape)} -> {tuple(c.shape)}")
+        arr[i] = _lib.Problem(m, n, k, a.data_ptr(), max(a.stride(0), k, 1), b.data_ptr(),
+                              max(b.stride(0), n, 1), c.data_ptr(), max(c.stride(0), n, 1))
+    return arr
+
+
+class GroupedPlan:
+    """A grouped product C_i = A_i @ B_i over many problems of uneven sizes,
+    planned once (tables in a workspace, launches captured in a CUDA graph)
+    and replayed with run(). The plan reads the tensors' current contents on
+    every run; keep them (and the plan) alive while it is used."""
+
+    def __init__(self, As, Bs, Cs=None, variant="ffma", config=None):
+        if Cs is None:
+            Cs = [torch.empty((a.shape[0], b.shape[1]), device=a.device) for a, b in zip(As, Bs)]
+        self.As, self.Bs, self.Cs = list(As), list(Bs), list(Cs)
+        self.variant = _variant(variant)
+        self._arr = _problems(self.As, self.Bs, self.Cs)
+        self._cfg = _config(config)
+        dev = self.As[0].device if self.As else torch.device("cuda")
+        with torch.cuda.device(dev):
+            need = int(lib().hbsg_grouped_workspace_size(len(self.As), self._arr, self.variant,
+                                                          self._cfg))
+            self.workspace = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+            torch.cuda.current_stream().synchronize()
+            self._plan = ctypes.c_void_p()
+            check(lib().hbsg_grouped_plan_create(ctypes.byref(self._plan), len(self.As), self._arr,
+                                                 self.variant, self._cfg,
+                                                 _ptr(self.workspace), need),
+                  "hbsg_grouped_plan_create")
+        self.device = dev
+
+    def run(self):
+        with torch.cuda.device(self.device):
+            check(lib().hbsg_grouped_run(self._plan, _stream()), "hbsg_grouped_run")
+        return self.Cs
+
+    def close(self):
+        if self._plan:
+            lib().hbsg_grouped_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gemm_grouped(As, Bs, Cs=None, variant="ffma", config=None, workspace=None):
+    """One-shot grouped product (tables built and uploaded per call, no graph)."""
+    if Cs is None:
+        Cs = [torch.empty((a.shape[0], b.shape[1]), device=a.device) for a, b in zip(As, Bs)]
+    arr = _problems(As, Bs, Cs)
+    v = _variant(variant)
+    cfgp = _config(config)
+    dev = As[0].device if len(As) else torch.device("cuda")
+    with torch.cuda.device(dev):
+        need = int(lib().hbsg_grouped_workspace_size(len(As), arr, v, cfgp))
+        ws = _workspace(max(need, 256), dev, workspace)
+        check(lib().hbsg_gemm_grouped(len(As), arr, v, cfgp, _ptr(ws), need, _stream()),
+              "hbsg_gemm_grouped")
+    return Cs
+
+
 def split_layout(m: int, n: int, k: int, variant="bf16x6") -> dict:
     """Byte offsets of the BF16 operand parts inside a split-BF16 workspace."""
     lay = _lib.SplitLayout()

@@ -137,6 +137,43 @@ typedef struct hbsg_split_layout {
 int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* out);
 
 /* ---------------------------------------------------------------------------
+ * Grouped GEMM: many independent row-major products C_i = A_i * B_i of uneven
+ * sizes in one persistent launch.
+ *
+ * Generalises the reference's NITER loop of independent products
+ * (apps/sgemm/kernel.cpp:293-297, all N x N) to per-problem M, N, K and
+ * strides, with the output tiles of all problems scheduled on one grid
+ * (cf. the grid-strided tile groups of
+ * apps/legacy/gemm/sgemm_group_cooperative/kernel.cpp:285-286).
+ *
+ * A plan lays its tables out in the caller's workspace, uploads them once
+ * (blocking copies) and captures the product's launches into a CUDA graph;
+ * hbsg_grouped_run replays the graph on a stream. The plan keeps the
+ * problems' pointers: rerun it whenever the operand contents change, and
+ * keep the workspace alive and untouched while the plan exists.
+ * hbsg_gemm_grouped builds the tables and launches directly (no graph).
+ */
+typedef struct hbsg_problem {
+    int m, n, k;
+    const float* a; int64_t lda;   /* m x k, row stride lda >= k */
+    const float* b; int64_t ldb;   /* k x n, row stride ldb >= n */
+    float* c; int64_t ldc;         /* m x n, row stride ldc >= n */
+} hbsg_problem;
+
+typedef struct hbsg_grouped_plan_s* hbsg_grouped_plan;
+
+size_t hbsg_grouped_workspace_size(int count, const hbsg_problem* problems, int variant,
+                                   const hbsg_config* cfg);
+int hbsg_grouped_plan_create(hbsg_grouped_plan* plan, int count, const hbsg_problem* problems,
+                             int variant, const hbsg_config* cfg,
+                             void* workspace, size_t workspace_bytes);
+int hbsg_grouped_run(hbsg_grouped_plan plan, hbsg_stream_t stream);
+int hbsg_grouped_plan_destroy(hbsg_grouped_plan plan);
+int hbsg_gemm_grouped(int count, const hbsg_problem* problems, int variant,
+                      const hbsg_config* cfg, void* workspace, size_t workspace_bytes,
+                      hbsg_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free split-BF16 GEMM. No counterpart in the reference.
  *
  * For callers that cannot allocate device memory at the moment they need a
