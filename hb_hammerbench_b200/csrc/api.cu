@@ -84,12 +84,34 @@ static SplitLayout split_layout(int M, int N, int K, int variant) {
 // Global tile ids: 1..F are the FFMA family, F+1..F+T the tensor-core family.
 static int total_tiles() { return ffma_num_tiles() + tc_num_tiles(); }
 
+// Tensor-core tile and K-slice count for a split-BF16 problem (shared by the
+// workspace query and the dispatcher so both agree). Returns false when an
+// explicitly requested tile does not fit the variant.
+static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg, int sms,
+                        int* tc, int* splits, int* kts) {
+  const int P = parts_of(variant);
+  const int tile = cfg && cfg->tile > 0 ? cfg->tile - 1 : -1;
+  if (tile >= 0) {
+    *tc = tile - ffma_num_tiles();
+    if (*tc < 0 || *tc >= tc_num_tiles() || tc_tile_parts(*tc) != P) return false;
+  } else {
+    *tc = tc_pick_tile(M, N, P, sms);
+  }
+  *splits = tc_pick_splits(*tc, M, N, K, cfg ? cfg->split_k : 0, sms, kts);
+  return true;
+}
+
 static size_t workspace_needed(int M, int N, int K, int batch, int variant, const hbsg_config* cfg) {
   if (variant == HBSG_FFMA) {
     const int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
     return ffma_workspace_bytes(M, N, batch, splits);
   }
-  return split_layout(M, N, K, variant).total;
+  int sms = current_device_sms(nullptr);
+  if (sms < 0) sms = 148;
+  int tc = 0, splits = 1, kts = 0;
+  if (!tc_schedule(M, N, K, variant, cfg, sms, &tc, &splits, &kts)) return 0;
+  const size_t partial = splits > 1 ? align256((size_t)splits * M * N * 4) : 0;
+  return split_layout(M, N, K, variant).total + partial;
 }
 
 // Core dispatcher for one (possibly batched) GEMM.
@@ -146,16 +168,11 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   // ---- split-BF16 on the tensor cores ----
   const int P = parts_of(variant);
   const bool scaled = scaled_of(variant);
-  int tc = -1;
-  if (tile >= 0) {
-    tc = tile - ffma_num_tiles();
-    if (tc < 0 || tc_tile_parts(tc) != P) return HBSG_ERR_UNSUPPORTED;
-  } else {
-    tc = tc_pick_tile(M, N, P, sms);
-  }
-  if (cfg && cfg->split_k > 1) return HBSG_ERR_UNSUPPORTED;
+  int tc = -1, splits = 1, kts = 0;
+  if (!tc_schedule(M, N, K, variant, cfg, sms, &tc, &splits, &kts)) return HBSG_ERR_UNSUPPORTED;
   const SplitLayout L = split_layout(M, N, K, variant);
-  if (!ws || ws_bytes < L.total || (reinterpret_cast<uintptr_t>(ws) & 255))
+  const size_t partial_bytes = splits > 1 ? align256((size_t)splits * M * N * 4) : 0;
+  if (!ws || ws_bytes < L.total + partial_bytes || (reinterpret_cast<uintptr_t>(ws) & 255))
     return HBSG_ERR_WORKSPACE;
   uint8_t* w = static_cast<uint8_t*>(ws);
   void* Ap = w + L.a_off;
@@ -181,7 +198,8 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
       if (e != cudaSuccess) return status_from(e);
     }
     if (flags & HBSG_FLAG_SPLIT_ONLY) continue;
-    e = tc_launch(tc, Ap, Bp, M, N, K, L.Kp, Cb, ldc, rowmax, colmax, raster, chunk, sms, 0, 0, st);
+    e = tc_launch(tc, Ap, Bp, M, N, K, L.Kp, Cb, ldc, rowmax, colmax, raster, chunk, sms, 0, 0, st,
+                  splits, reinterpret_cast<float*>(w + L.total));
     if (e != cudaSuccess) return status_from(e);
   }
   return HBSG_OK;

@@ -189,12 +189,31 @@ cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st) 
   dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)p.splits, (unsigned)batch);
   cudaError_t err = e.launch(p, grid, st, vec);
   if (err != cudaSuccess || p.splits == 1) return err;
-  const long total = (long)p.M * p.N * batch;
-  long nb = (total + 255) / 256;
-  int blocks = (int)(nb < 148L * 16 ? nb : 148L * 16);
-  splitk_reduce_kernel<<<blocks, 256, 0, st>>>(p.partial, p.C, p.M, p.N, p.ldc, p.strideC,
-                                               p.splits, batch);
+  return splitk_reduce(p.partial, p.C, p.M, p.N, p.ldc, p.strideC, p.splits, batch, 148, st);
+}
+
+cudaError_t splitk_reduce(const float* partial, float* C, int M, int N, long ldc, long strideC,
+                          int splits, int batches, int sms, cudaStream_t st) {
+  const long total = (long)M * N * batches;
+  const long nb = (total + 255) / 256;
+  const long cap = (long)sms * 16;
+  const int blocks = (int)(nb < cap ? nb : cap);
+  splitk_reduce_kernel<<<blocks, 256, 0, st>>>(partial, C, M, N, ldc, strideC, splits, batches);
   return cudaGetLastError();
+}
+
+// Split count for the FFMA kernel: the requested count, or (0) enough K
+// slices to fill every SM when the output has too few tiles, keeping at least
+// 16 k-tiles (256 of K) per slice.
+int ffma_pick_splits(int tile_idx, int M, int N, int K, int batch, int requested, int sms) {
+  if (requested > 0) return requested;
+  const FfmaEntry& e = kFfmaTiles[tile_idx];
+  const long tiles = (long)((M + e.bm - 1) / e.bm) * ((N + e.bn - 1) / e.bn) * batch;
+  const long slots = (long)sms * (e.threads <= 128 ? 2 : 1);
+  if (tiles * 2 > slots) return 1;
+  const long by_k = K / (16 * e.bk) > 1 ? K / (16 * e.bk) : 1;
+  const long s = (slots + tiles - 1) / tiles;
+  return (int)(s < by_k ? s : by_k);
 }
 
 }  // namespace hbsg

@@ -68,6 +68,7 @@ struct GTiles {  // tile source for the tensor-core body
     w.N = p.N;
     w.m0 = e.y;
     w.n0 = e.z;
+    w.kt0 = 0;
     w.KT = p.Kp / kBK;
     w.rowmax = p.rowmax;
     w.colmax = p.colmax;

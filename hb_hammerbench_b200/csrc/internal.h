@@ -43,7 +43,13 @@ int tc_pick_tile(int M, int N, int parts, int sms);
 cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,
                       float* C, long ldc, const uint32_t* rowmax, const uint32_t* colmax,
                       int raster, int chunk_k, int sms, int debug_skip_loads,
-                      unsigned long long wait_limit_ns, cudaStream_t st);
+                      unsigned long long wait_limit_ns, cudaStream_t st, int splits = 1,
+                      float* partial = nullptr);
+int tc_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split);
+int ffma_pick_splits(int tile_idx, int M, int N, int K, int batch, int requested, int sms);
+// C[b] = sum over s of partial[b][s] (fixed order), partial rows of N floats.
+cudaError_t splitk_reduce(const float* partial, float* C, int M, int N, long ldc, long strideC,
+                          int splits, int batches, int sms, cudaStream_t st);
 int tc_read_and_clear_device_error();
 int grouped_read_and_clear_device_error();
 int tc_chunk_ktiles(int parts, int chunk_k);

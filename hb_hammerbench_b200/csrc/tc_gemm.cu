@@ -25,6 +25,8 @@
 // No TMA multicast is used; every CTA fetches its own tiles.
 // Every wait is bounded: after kWaitLimitNs the kernel records
 // HBSG_ERR_DEVICE_TIMEOUT in the device error flag and unwinds.
+#include <algorithm>
+
 #include "tc_kernel.cuh"
 
 namespace hbsg {
@@ -33,7 +35,9 @@ struct TcParams {
   int M, N, K, Kp;
   int tiles_m, tiles_n, num_tiles;
   int raster;
-  float* C;
+  int splits;        // K slices (1 = none)
+  int kt_per_split;  // k-tiles per slice
+  float* C;          // output, or the slice partials [splits][M][N] when splits > 1
   long ldc;
   const uint32_t* rowmax;  // null unless scaled
   const uint32_t* colmax;
@@ -46,8 +50,13 @@ struct SingleTiles {
   const CUtensorMap* ma;
   const CUtensorMap* mb;
   const TcParams* p;
+  // Work item t = slice * num_tiles + tile: with split-K the slices of all
+  // tiles are independent items; slice s covers k-tiles [s*kts, (s+1)*kts)
+  // and writes its partial to C + s*M*N (row stride N).
   template <int BN>
-  __device__ __forceinline__ TileWork get_bn(int t) const {
+  __device__ __forceinline__ TileWork get_bn(int item) const {
+    const int slice = item / p->num_tiles;
+    const int t = item - slice * p->num_tiles;
     const int span = p->raster * p->tiles_n;
     const int g = t / span;
     const int first = g * p->raster;
@@ -56,13 +65,20 @@ struct SingleTiles {
     TileWork w;
     w.ma = ma;
     w.mb = mb;
-    w.C = p->C;
-    w.ldc = p->ldc;
     w.M = p->M;
     w.N = p->N;
     w.m0 = (first + in % gm) * kBM;
     w.n0 = (in / gm) * BN;
-    w.KT = p->Kp / kBK;
+    const int KT = p->Kp / kBK;
+    w.kt0 = slice * p->kt_per_split;
+    w.KT = min(p->kt_per_split, KT - w.kt0);
+    if (p->splits > 1) {
+      w.C = p->C + (long)slice * p->M * p->N;
+      w.ldc = p->N;
+    } else {
+      w.C = p->C;
+      w.ldc = p->ldc;
+    }
     w.rowmax = p->rowmax;
     w.colmax = p->colmax;
     return w;
@@ -71,7 +87,7 @@ struct SingleTiles {
 
 template <int BN>
 struct SingleTilesBN : SingleTiles {
-  __device__ __forceinline__ int count() const { return p->num_tiles; }
+  __device__ __forceinline__ int count() const { return p->num_tiles * p->splits; }
   __device__ __forceinline__ TileWork get(int t) const { return get_bn<BN>(t); }
 };
 
@@ -189,10 +205,31 @@ int tc_pick_tile(int M, int N, int parts, int sms) {
   return best;
 }
 
+// Number of K slices for a problem: the requested count, or (0) enough slices
+// to give every SM a work item when the output has too few tiles, keeping at
+// least 8 k-tiles (256 of K) per slice. Returns the count actually used (no
+// empty slices) and the k-tiles per slice.
+int tc_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
+  const TcEntry& e = kTcTiles[idx];
+  const int KT = ((K + 31) / 32 * 32) / kBK > 0 ? ((K + 31) / 32 * 32) / kBK : 1;
+  const long tiles = (long)((M + kBM - 1) / kBM) * ((N + e.bn - 1) / e.bn);
+  int s = requested;
+  if (s <= 0) {
+    s = 1;
+    if (tiles * 2 <= sms) s = (int)std::min<long>((sms + tiles - 1) / tiles, std::max(1, KT / 8));
+  }
+  s = std::max(1, std::min(s, KT));
+  int per = (KT + s - 1) / s;
+  s = (KT + per - 1) / per;
+  *kt_per_split = per;
+  return s;
+}
+
 cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,
                       float* C, long ldc, const uint32_t* rowmax, const uint32_t* colmax,
                       int raster, int chunk_k, int sms, int debug_skip_loads,
-                      unsigned long long wait_limit_ns, cudaStream_t st) {
+                      unsigned long long wait_limit_ns, cudaStream_t st, int splits,
+                      float* partial) {
   const TcEntry& e = kTcTiles[idx];
   CUtensorMap ma, mb;
   if (!tc_make_parts_map_impl(&ma, Ap, e.parts, M, Kp, kBM)) return cudaErrorInvalidValue;
@@ -206,16 +243,22 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
   p.tiles_n = (N + e.bn - 1) / e.bn;
   p.num_tiles = p.tiles_m * p.tiles_n;
   p.raster = raster > 0 ? raster : 16;
-  p.C = C;
-  p.ldc = ldc;
+  int kts = Kp / kBK;
+  p.splits = splits > 1 ? tc_pick_splits(idx, M, N, K, splits, sms, &kts) : 1;
+  p.kt_per_split = kts;
+  p.C = p.splits > 1 ? partial : C;
+  p.ldc = p.splits > 1 ? N : ldc;
   p.rowmax = rowmax;
   p.colmax = colmax;
   TcRun run;
   run.chunk_ktiles = tc_chunk_ktiles(e.parts, chunk_k);
   run.debug_skip_loads = debug_skip_loads;
   run.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;
-  const int grid = p.num_tiles < sms ? p.num_tiles : sms;
-  return e.launch(ma, mb, p, run, grid, st, rowmax != nullptr);
+  const long items = (long)p.num_tiles * p.splits;
+  const int grid = (int)(items < sms ? items : sms);
+  cudaError_t err = e.launch(ma, mb, p, run, grid, st, rowmax != nullptr);
+  if (err != cudaSuccess || p.splits == 1) return err;
+  return splitk_reduce(partial, C, M, N, ldc, 0, p.splits, 1, sms, st);
 }
 
 // Default drain interval: every k-tile for the 6-product form (its error is

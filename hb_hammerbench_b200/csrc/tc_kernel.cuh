@@ -152,6 +152,24 @@ struct TcShape {
   static_assert(BN % 16 == 0 && BN >= 64 && BN <= 256, "UMMA N");
 };
 
+// frexp exponent of max|x| from its FP32 bit pattern: the scale 2^-e the
+// split applied to that row or column (0 for zero, non-finite or absent).
+HBSG_DEV int pow2_exp_of_bits(uint32_t bits) {
+  const int E = (int)((bits >> 23) & 0xffu);
+  if (E == 0xff || bits == 0u) return 0;
+  if (E != 0) return E - 126;
+  int e;
+  frexpf(__uint_as_float(bits), &e);  // subnormal maximum
+  return e;
+}
+
+// x * 2^s, exact when 2^s is a normal float (one rounding otherwise, as ldexpf).
+HBSG_DEV float scale_pow2(float x, int s) {
+  if (s == 0) return x;
+  if (s >= -126 && s <= 127) return x * __uint_as_float((uint32_t)(s + 127) << 23);
+  return ldexpf(x, s);
+}
+
 // One output tile of work for the kernel body.
 struct TileWork {
   const CUtensorMap* ma;  // A parts map (box {32, 128, P})
@@ -160,7 +178,8 @@ struct TileWork {
   long ldc;
   int M, N;
   int m0, n0;
-  int KT;  // k-tiles of 32
+  int kt0;  // first k-tile (of 32) of this work item
+  int KT;   // k-tiles in this work item
   const uint32_t* rowmax;  // scaled forms only
   const uint32_t* colmax;
 };
@@ -241,8 +260,8 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           const uint32_t sa = base + s * S::kStageBytes;
           const uint32_t sb = sa + P * S::kABytes;
           mbar_arrive_expect_tx(&full[s], S::kStageBytes);
-          tma_load_3d(sa, w.ma, kt * kBK, w.m0, 0, &full[s]);
-          tma_load_3d(sb, w.mb, kt * kBK, w.n0, 0, &full[s]);
+          tma_load_3d(sa, w.ma, (w.kt0 + kt) * kBK, w.m0, 0, &full[s]);
+          tma_load_3d(sb, w.mb, (w.kt0 + kt) * kBK, w.n0, 0, &full[s]);
         }
       }
     }
@@ -332,10 +351,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
       if (row < w.M) {
         float* crow = w.C + (long)row * w.ldc;
         int er = 0;
-        if constexpr (SCALED) {
-          const float mx = __uint_as_float(w.rowmax[row]);
-          if (mx > 0.0f && isfinite(mx)) frexpf(mx, &er);
-        }
+        if constexpr (SCALED) er = pow2_exp_of_bits(w.rowmax[row]);
         const bool vec = ((w.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(w.C) & 15) == 0);
 #pragma unroll
         for (int j = 0; j < COLS; j += 4) {
@@ -345,10 +361,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
             float x = sum[j + e];
             if constexpr (SCALED) {
               const int cc = min(col0 + j + e, w.N - 1);
-              const float mx = __uint_as_float(w.colmax[cc]);
-              int ec = 0;
-              if (mx > 0.0f && isfinite(mx)) frexpf(mx, &ec);
-              x = ldexpf(x, er + ec);
+              x = scale_pow2(x, er + pow2_exp_of_bits(w.colmax[cc]));
             }
             o[e] = x;
           }

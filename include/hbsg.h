@@ -50,7 +50,10 @@ typedef enum hbsg_variant {
  * heuristic". */
 typedef struct hbsg_config {
     int tile;          /* tile-shape id, 1-based index into hbsg_tile_info (0 = heuristic) */
-    int split_k;       /* number of K slices (0/1 = none); slices are reduced in fixed order */
+    int split_k;       /* K slices, reduced in fixed order. FFMA: 0/1 = none (keeps the one
+                          sequential FMA chain per output), n > 1 = n slices. Split-BF16:
+                          0 = library heuristic (slices only when the output has too few
+                          tiles to fill the GPU), 1 = none, n > 1 = n slices. */
     int raster_group;  /* tile rows per rasterisation group (0 = heuristic) */
     int chunk_k;       /* split-BF16: K elements accumulated on the tensor core before the
                           partial is added in FP32 registers (0 = heuristic) */
@@ -186,7 +189,7 @@ int hbsg_gemm_grouped(int count, const hbsg_problem* problems, int variant,
  * the library: HBSG_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory that
  * every GPU which loads the library holds until the process exits.
  *
- *   - Problems whose split workspace (hbsg_get_split_layout().total_bytes)
+ *   - Problems whose workspace (hbsg_gemm_workspace_size with no config)
  *     exceeds HBSG_NOALLOC_SCRATCH_BYTES are rejected with
  *     HBSG_ERR_WORKSPACE before anything is launched. M = N = K = 1024 with
  *     BF16X6 needs 12.6 MB and fits.

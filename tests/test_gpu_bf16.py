@@ -233,3 +233,29 @@ def test_device_wait_timeout_is_reported_and_recoverable(hb):
     A = _rand((256, 256), 71)
     B = _rand((256, 256), 72)
     assert _err(hb.gemm(A, B, variant="bf16x6"), A.double() @ B.double())[0] < 2e-6
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
+@pytest.mark.parametrize("m,n,k,splits", [(256, 256, 65536, 0), (128, 256, 20000, 7), (300, 100, 4096, 3)])
+def test_split_k(hb, variant, m, n, k, splits):
+    import torch
+    A = _rand((m, k), k + 1)
+    B = _rand((k, n), k + 2)
+    ref = A.double() @ B.double()
+    cfg = {"split_k": splits}
+    C1 = hb.gemm(A, B, variant=variant, config=cfg)
+    C2 = hb.gemm(A, B, variant=variant, config=cfg)
+    assert torch.equal(C1, C2)  # fixed reduction order: deterministic
+    e = _err(C1, ref)
+    e1 = _err(hb.gemm(A, B, variant=variant, config={"split_k": 1}), ref)
+    bound = 2.0 ** -16 if "x3" in variant else 1e-6
+    assert e[0] < bound and e1[0] < bound * 4, (e, e1)
+    if "x6" in variant:
+        assert e[0] <= _err(hb.gemm(A, B), ref)[0]  # no worse than FFMA
+
+
+def test_split_k_workspace_reported(hb):
+    m, n, k = 256, 256, 1 << 16
+    need_auto = hb.gemm_workspace_size(m, n, k, "bf16x6")
+    need_one = hb.gemm_workspace_size(m, n, k, "bf16x6", config={"split_k": 1})
+    assert need_auto > need_one  # the heuristic splits this shape (2 tiles)
