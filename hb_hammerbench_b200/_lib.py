@@ -36,7 +36,7 @@ class Config(ctypes.Structure):
     """struct hbsg_config"""
     _fields_ = [("tile", ctypes.c_int), ("split_k", ctypes.c_int),
                 ("raster_group", ctypes.c_int), ("chunk_k", ctypes.c_int),
-                ("flags", ctypes.c_int)]
+                ("flags", ctypes.c_int), ("inline_split_pct", ctypes.c_int)]
 
 
 FLAG_PRESPLIT_A = 1

@@ -50,9 +50,13 @@ struct GProblem {  // one problem, as the kernels see it
   uint32_t* colmax;
 };
 
-struct GTiles {  // tile source for the tensor-core body
+struct GTiles {  // tile source for the tensor-core body (split pass run beforehand)
+  static constexpr bool kInlineSplit = false;
+  __device__ bool wait_ready(int, int, volatile int*, unsigned long long) const { return true; }
+  template <int P, bool SCALED>
+  __device__ void split_worker(int, volatile int*) const {}
   const GProblem* probs;
-  const int4* tiles;  // {problem, m0, n0, 0}
+  const int4* tiles;  // {problem, m0, n0, inline-split jobs of the problem (0 = split before)}
   const CUtensorMap* maps;  // 2 per problem: A parts, B parts
   int n;
   __device__ __forceinline__ int count() const { return n; }
@@ -60,6 +64,8 @@ struct GTiles {  // tile source for the tensor-core body
     const int4 e = tiles[t];
     const GProblem& p = probs[e.x];
     TileWork w;
+    w.prob = e.x;
+    w.ready_target = e.w;
     w.ma = maps + 2 * e.x;
     w.mb = maps + 2 * e.x + 1;
     w.C = p.C;
@@ -78,6 +84,246 @@ struct GTiles {  // tile source for the tensor-core body
 
 template <int P, int BN, int STAGES, bool SCALED>
 __global__ void __launch_bounds__(320, 1) tc_grouped_kernel(const GTiles tiles, const TcRun run) {
+  tc_body<P, BN, STAGES, SCALED>(tiles, run);
+}
+
+// ---- inline split --------------------------------------------------------------
+// The split of the operands into BF16 parts runs inside the tensor-core
+// kernel, on two extra warps per CTA, while the tensor cores work on earlier
+// problems. Work is cut into jobs of 32 x 32 operand elements, numbered in
+// the problems' tile order (A jobs then B jobs per problem); splitter warps
+// claim jobs from a global counter (so progress never depends on which CTAs
+// are resident) and count finished jobs per problem. A CTA's TMA producer
+// loads a problem's first tile only after that count is complete. Splitters
+// wait on nothing, so the dependency chain always ends.
+struct SplitJob {
+  int valid, isA, r0, k0;
+};
+
+// The problem a splitter warp is working on, cached in registers: claims are
+// mostly consecutive within one problem, so the job-to-problem search (a
+// chain of dependent global loads) is only repeated when a claim leaves it.
+struct SplitCursor {
+  int first = 0, last = -1;  // job range [first, last) of the cached problem
+  int prob = -1;
+  const float* A;
+  const float* B;
+  long lda, ldb;
+  int M, N, K, Kp, kb, na, nb;
+  __nv_bfloat16* Ap;
+  __nv_bfloat16* Bp;
+  const uint32_t* rowmax;
+  const uint32_t* colmax;
+};
+
+struct GTilesInline : GTiles {
+  static constexpr bool kInlineSplit = true;
+  int* ready;            // finished jobs per problem (zeroed before the launch)
+  int* job_counter;      // next unclaimed job (zeroed before the launch)
+  const int* order;      // problem index of the i-th problem in tile order
+  const int* job_start;  // first job of the i-th problem in tile order; [count] = total
+  const int* jobs_of;    // jobs per problem
+  int num_problems;
+  int num_jobs;
+
+  __device__ __forceinline__ bool wait_ready(int prob, int target, volatile int* abort_flag,
+                                             unsigned long long limit_ns) const {
+    const int* addr = ready + prob;
+    const unsigned long long t0 = globaltimer();
+    for (uint32_t i = 0;; ++i) {
+      int v;
+      asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(addr) : "memory");
+      if (v >= target) break;
+      if (*abort_flag) return false;
+      if ((i & 15) == 15 && globaltimer() - t0 > limit_ns) {
+        *abort_flag = 1;
+        atomicExch(&g_device_error, (int)HBSG_ERR_DEVICE_TIMEOUT);
+        return false;
+      }
+      __nanosleep(64);
+    }
+    // the parts were written through the generic proxy; the TMA reads them
+    // through the async proxy
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    return true;
+  }
+
+  __device__ __forceinline__ void seek(SplitCursor& c, int j) const {
+    int lo = 0, hi = num_problems;  // largest i with job_start[i] <= j
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(job_start + mid) <= j) lo = mid;
+      else hi = mid;
+    }
+    const int p = __ldg(order + lo);
+    const GProblem& g = probs[p];
+    c.first = __ldg(job_start + lo);
+    c.last = __ldg(job_start + lo + 1);
+    c.prob = p;
+    c.A = g.A;
+    c.B = g.B;
+    c.lda = g.lda;
+    c.ldb = g.ldb;
+    c.M = g.M;
+    c.N = g.N;
+    c.K = g.K;
+    c.Kp = g.Kp;
+    c.kb = g.Kp / 32;
+    c.na = ((g.M + 31) / 32) * c.kb;
+    c.nb = (g.N + 31) / 32;
+    c.Ap = static_cast<__nv_bfloat16*>(g.Ap);
+    c.Bp = static_cast<__nv_bfloat16*>(g.Bp);
+    c.rowmax = g.rowmax;
+    c.colmax = g.colmax;
+  }
+
+  __device__ __forceinline__ SplitJob decode(const SplitCursor& c, int j) const {
+    SplitJob d{};
+    d.valid = 1;
+    int local = j - c.first;
+    if (local < c.na) {
+      d.isA = 1;
+      d.r0 = (local / c.kb) * 32;
+      d.k0 = (local % c.kb) * 32;
+    } else {
+      local -= c.na;
+      d.isA = 0;
+      d.r0 = (local % c.nb) * 32;
+      d.k0 = (local / c.nb) * 32;
+    }
+    return d;
+  }
+
+  // Lane l loads row r0 + l of A (32 consecutive k), or column r0 + l of B
+  // (32 consecutive k, each load instruction coalesced across the warp).
+  __device__ __forceinline__ void load(const SplitCursor& c, const SplitJob& d, int lane,
+                                       float* v) const {
+    const int r = d.r0 + lane;
+    if (d.isA) {
+      if (r >= c.M) return;
+      const float* src = c.A + (long)r * c.lda + d.k0;
+      if (d.k0 + 32 <= c.K && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float4 x = __ldg(reinterpret_cast<const float4*>(src + 4 * i));
+          v[4 * i] = x.x;
+          v[4 * i + 1] = x.y;
+          v[4 * i + 2] = x.z;
+          v[4 * i + 3] = x.w;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = (d.k0 + i < c.K) ? __ldg(src + i) : 0.0f;
+      }
+    } else {
+      const bool in = r < c.N;
+      const float* src = c.B + (long)d.k0 * c.ldb + r;
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        v[i] = (in && d.k0 + i < c.K) ? __ldg(src + (long)i * c.ldb) : 0.0f;
+    }
+  }
+
+  template <int P, bool SCALED>
+  __device__ __forceinline__ void store(const SplitCursor& c, const SplitJob& d, int lane,
+                                        const float* v) const {
+    const int r = d.r0 + lane;
+    const int rows = d.isA ? c.M : c.N;
+    if (r >= rows) return;
+    int e = 0;
+    if constexpr (SCALED) e = exp_from_maxbits(d.isA ? c.rowmax[r] : c.colmax[r]);
+    const long plane = (long)rows * c.Kp;
+    __nv_bfloat16* dst = (d.isA ? c.Ap : c.Bp) + (long)r * c.Kp + d.k0;
+#pragma unroll
+    for (int gi = 0; gi < 4; ++gi) {
+      __align__(16) __nv_bfloat16 parts[P][8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        __nv_bfloat16 o[3];
+        split_value<P>(v[8 * gi + i], e, o);
+#pragma unroll
+        for (int q = 0; q < P; ++q) parts[q][i] = o[q];
+      }
+#pragma unroll
+      for (int q = 0; q < P; ++q)
+        *reinterpret_cast<uint4*>(dst + q * plane + 8 * gi) = *reinterpret_cast<const uint4*>(parts[q]);
+    }
+  }
+
+  // L2 prefetch of the source lines of job j (lane l: A row r0 + l, or B row
+  // k0 + l of the job's 32 columns): 128 bytes per lane.
+  __device__ __forceinline__ void prefetch(SplitCursor& c, int j, int lane) const {
+    if (j >= num_jobs) return;
+    if (j < c.first || j >= c.last) seek(c, j);
+    const SplitJob d = decode(c, j);
+    const float* src = nullptr;
+    if (d.isA) {
+      const int r = d.r0 + lane;
+      if (r < c.M && d.k0 < c.K) src = c.A + (long)r * c.lda + d.k0;
+    } else {
+      const int k = d.k0 + lane;
+      if (k < c.K && d.r0 < c.N) src = c.B + (long)k * c.ldb + d.r0;
+    }
+    if (src) asm volatile("prefetch.global.L2 [%0];" ::"l"(src));
+  }
+
+  template <int P, bool SCALED>
+  __device__ __forceinline__ void split_worker(int lane, volatile int* abort_flag) const {
+    constexpr int BATCH = 2;  // jobs loaded together (64 loads in flight per lane)
+    SplitCursor cur, pcur;
+    int next = 0;
+    if (lane == 0) next = atomicAdd(job_counter, BATCH);
+    next = __shfl_sync(0xffffffffu, next, 0);
+#pragma unroll
+    for (int b = 0; b < BATCH; ++b) prefetch(pcur, next + b, lane);
+    for (;;) {
+      if (*abort_flag) return;
+      const int j0 = next;
+      if (j0 >= num_jobs) return;
+      // claim the following batch now; the atomic's latency overlaps this batch
+      if (lane == 0) next = atomicAdd(job_counter, BATCH);
+      SplitJob d[BATCH];
+      int prob[BATCH];
+      float v[BATCH][32];
+#pragma unroll
+      for (int b = 0; b < BATCH; ++b) {
+        const int j = j0 + b;
+        d[b].valid = 0;
+        prob[b] = -1;
+        if (j >= num_jobs) continue;
+        if (j < cur.first || j >= cur.last) seek(cur, j);
+        d[b] = decode(cur, j);
+        prob[b] = cur.prob;
+        load(cur, d[b], lane, v[b]);
+      }
+      // pull the following batch's source lines into L2 while this one is
+      // in flight, so its loads hit L2
+      next = __shfl_sync(0xffffffffu, next, 0);
+#pragma unroll
+      for (int b = 0; b < BATCH; ++b) prefetch(pcur, next + b, lane);
+#pragma unroll
+      for (int b = 0; b < BATCH; ++b) {
+        if (!d[b].valid) continue;
+        const int j = j0 + b;
+        if (j < cur.first || j >= cur.last) seek(cur, j);
+        store<P, SCALED>(cur, d[b], lane, v[b]);
+      }
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+#pragma unroll
+        for (int b = 0; b < BATCH; ++b)
+          if (prob[b] >= 0)
+            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(ready + prob[b]) : "memory");
+      }
+    }
+  }
+};
+
+template <int P, int BN, int STAGES, bool SCALED>
+__global__ void __launch_bounds__(384, 1)
+    tc_grouped_inline_kernel(const GTilesInline tiles, const TcRun run) {
   tc_body<P, BN, STAGES, SCALED>(tiles, run);
 }
 
@@ -139,7 +385,8 @@ __global__ void __launch_bounds__(256) gsplit_a_kernel(const GProblem* __restric
   }
 }
 
-// B: job {problem, k0, n0, 0}: one 64 x 64 block transposed into [N][Kp].
+// B: job {problem, k0, n0, 0}: one 64 x 64 block transposed through shared
+// memory into [N][Kp] (8 threads write each 128-byte output row segment).
 template <int P, bool SCALED>
 __global__ void __launch_bounds__(256) gsplit_b_kernel(const GProblem* __restrict__ probs,
                                                        const int4* __restrict__ jobs) {
@@ -195,14 +442,17 @@ static int parts_of_v(int v) { return (v == HBSG_BF16X6 || v == HBSG_BF16X6_SCAL
 static bool scaled_of_v(int v) { return v == HBSG_BF16X3_SCALED || v == HBSG_BF16X6_SCALED; }
 
 struct GLayout {
-  size_t probs_off, tiles_off, maps_off, jobs_off, parts_off, max_off, total;
+  size_t probs_off, tiles_off, maps_off, jobs_off, sync_off, parts_off, max_off, total;
   long num_tiles, num_jobs_a, num_jobs_b, num_jobs_rmax, num_jobs_cmax;
+  long inline_jobs;  // 32 x 32 split jobs of the inline split (0 when split separately)
   size_t colmax_bytes;
+  size_t sync_bytes;  // ready[count] + job counter (zeroed per run), then order, job_start, jobs_of
 };
 
 struct GroupedPlan {
   int variant;
   int count;
+  bool inline_split;
   int ffma_tile;  // index into the FFMA table, or -1
   int tc_tile;    // index into the tensor-core table, or -1
   GLayout L;
@@ -214,8 +464,59 @@ struct GroupedPlan {
   cudaGraphExec_t exec = nullptr;
 };
 
+// Default share of the split work (in jobs) done inside the product kernel:
+// none. Measured on B200 with the 512-problem batch (M, N, K in 64..2048),
+// moving 20-60 % of the split onto two extra warps per CTA made the product
+// slower than splitting everything beforehand (the tensor-core pipeline loses
+// more than the overlap gains), so the inline split is opt-in.
+static constexpr int kDefaultInlinePct = -1;
+
+static int kp_of(int k) { return std::max(32, (k + 31) / 32 * 32); }
+
+// 32 x 32 split jobs of one problem (A then B).
+static long inline_jobs_of(const hbsg_problem& q) {
+  if (q.m <= 0 || q.n <= 0) return 0;
+  const int Kp = kp_of(q.k);
+  return (long)((q.m + 31) / 32) * (Kp / 32) + (long)(Kp / 32) * ((q.n + 31) / 32);
+}
+
+// Problems in tile order (K descending, stable) and which of them the
+// product kernel splits itself: the problems processed last, holding about
+// `pct` percent of the split jobs. The others are split by separate kernels
+// before the product starts.
+struct GSets {
+  std::vector<int> order;
+  std::vector<char> inl;
+  bool any_inline = false;
+};
+
+static GSets grouped_sets(int count, const hbsg_problem* pr, int variant, const hbsg_config* cfg) {
+  GSets S;
+  S.order.resize(count);
+  std::iota(S.order.begin(), S.order.end(), 0);
+  std::stable_sort(S.order.begin(), S.order.end(),
+                   [&](int x, int y) { return pr[x].k > pr[y].k; });
+  S.inl.assign(count, 0);
+  int pct = cfg && cfg->inline_split_pct != 0 ? cfg->inline_split_pct : kDefaultInlinePct;
+  if (variant == HBSG_FFMA || pct < 0) pct = 0;
+  pct = std::min(pct, 100);
+  long total = 0;
+  for (int i = 0; i < count; ++i) total += inline_jobs_of(pr[i]);
+  const long target = total * pct / 100;
+  long acc = 0;
+  for (int i = count - 1; i >= 0 && acc < target; --i) {
+    const int p = S.order[i];
+    acc += inline_jobs_of(pr[p]);
+    S.inl[p] = 1;
+    S.any_inline = true;
+  }
+  return S;
+}
+
 // Tile counts and job counts for a problem set (host arrays).
-static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, int bm, int bn) {
+static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, int bm, int bn,
+                              const GSets& sets) {
+  const bool inline_split = sets.any_inline;
   GLayout L{};
   const bool split = variant != HBSG_FFMA;
   const int P = split ? parts_of_v(variant) : 0;
@@ -226,11 +527,15 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
     if (q.m <= 0 || q.n <= 0) continue;
     L.num_tiles += (long)((q.m + bm - 1) / bm) * ((q.n + bn - 1) / bn);
     if (split) {
-      const int Kp = std::max(32, (q.k + 31) / 32 * 32);
+      const int Kp = kp_of(q.k);
       parts += al((size_t)P * q.m * Kp * 2, 256) + al((size_t)P * q.n * Kp * 2, 256);
-      const long units = (long)q.m * (Kp / 8);
-      L.num_jobs_a += (units + 2047) / 2048;
-      L.num_jobs_b += (long)((Kp + 63) / 64) * ((q.n + 63) / 64);
+      if (sets.inl[i]) {
+        L.inline_jobs += inline_jobs_of(q);
+      } else {
+        const long units = (long)q.m * (Kp / 8);
+        L.num_jobs_a += (units + 2047) / 2048;
+        L.num_jobs_b += (long)((Kp + 63) / 64) * ((q.n + 63) / 64);
+      }
       if (scaled) {
         maxes += al((size_t)q.m * 4, 256);
         cmax += al((size_t)q.n * 4, 256);
@@ -244,7 +549,10 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
   L.maps_off = al(L.tiles_off + sizeof(int4) * (size_t)L.num_tiles, 256);
   L.jobs_off = al(L.maps_off + (split ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
   const long jobs = L.num_jobs_a + L.num_jobs_b + L.num_jobs_rmax + L.num_jobs_cmax;
-  L.parts_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);
+  L.sync_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);
+  L.sync_bytes = inline_split ? al(sizeof(int) * ((size_t)count + 1), 256) : 0;
+  const size_t sync_tables = inline_split ? al(sizeof(int) * (3 * (size_t)count + 1), 256) : 0;
+  L.parts_off = al(L.sync_off + L.sync_bytes + sync_tables, 256);
   L.max_off = L.parts_off + parts;
   L.colmax_bytes = cmax;
   L.total = L.max_off + cmax + maxes;  // colmax block first (one memset), then rowmax
@@ -321,6 +629,12 @@ struct GTcEntry {
            reinterpret_cast<const void*>(&tc_grouped_kernel<P, BN, ST, false>),          \
            reinterpret_cast<const void*>(&tc_grouped_kernel<P, BN, ST, true>)},
 static const GTcEntry kGTc[] = {HBSG_TC_TILE_LIST(HBSG_GTC_ENTRY)};
+#define HBSG_GTCI_ENTRY(P, BN, ST)                                                          \
+  GTcEntry{TcShape<P, BN, ST>::kSmemBytes,                                                  \
+           reinterpret_cast<const void*>(&tc_grouped_inline_kernel<P, BN, ST, false>),      \
+           reinterpret_cast<const void*>(&tc_grouped_inline_kernel<P, BN, ST, true>)},
+static const GTcEntry kGTcInline[] = {HBSG_TC_TILE_LIST(HBSG_GTCI_ENTRY)};
+static uint32_t g_tci_masks[sizeof(kGTcInline) / sizeof(kGTcInline[0])][2];
 
 static uint32_t g_ffma_masks[9][2];
 static uint32_t g_tc_masks[sizeof(kGTc) / sizeof(kGTc[0])][2];
@@ -364,26 +678,46 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
     }
   }
   if (L.num_jobs_b) {
+    const unsigned nb = (unsigned)L.num_jobs_b;
     if (P == 3) {
-      if (scaled) gsplit_b_kernel<3, true><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
-      else gsplit_b_kernel<3, false><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
+      if (scaled) gsplit_b_kernel<3, true><<<nb, 256, 0, st>>>(probs, jb);
+      else gsplit_b_kernel<3, false><<<nb, 256, 0, st>>>(probs, jb);
     } else {
-      if (scaled) gsplit_b_kernel<2, true><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
-      else gsplit_b_kernel<2, false><<<(unsigned)L.num_jobs_b, 256, 0, st>>>(probs, jb);
+      if (scaled) gsplit_b_kernel<2, true><<<nb, 256, 0, st>>>(probs, jb);
+      else gsplit_b_kernel<2, false><<<nb, 256, 0, st>>>(probs, jb);
     }
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const GTcEntry& te = kGTc[pl.tc_tile];
-  const void* k = scaled ? te.k1 : te.k0;
-  if (!set_smem_once(k, te.smem, &g_tc_masks[pl.tc_tile][scaled ? 1 : 0]))
-    return cudaErrorInvalidValue;
   GTiles gt;
   gt.probs = probs;
   gt.tiles = tiles;
   gt.maps = reinterpret_cast<const CUtensorMap*>(pl.ws + L.maps_off);
   gt.n = (int)L.num_tiles;
   TcRun run = pl.run;
+  if (pl.inline_split) {
+    e = cudaMemsetAsync(pl.ws + L.sync_off, 0, L.sync_bytes, st);
+    if (e != cudaSuccess) return e;
+    const GTcEntry& te = kGTcInline[pl.tc_tile];
+    const void* k = scaled ? te.k1 : te.k0;
+    if (!set_smem_once(k, te.smem, &g_tci_masks[pl.tc_tile][scaled ? 1 : 0]))
+      return cudaErrorInvalidValue;
+    GTilesInline gi;
+    static_cast<GTiles&>(gi) = gt;
+    gi.ready = reinterpret_cast<int*>(pl.ws + L.sync_off);
+    gi.job_counter = gi.ready + pl.count;
+    gi.order = reinterpret_cast<const int*>(pl.ws + L.sync_off + L.sync_bytes);
+    gi.job_start = gi.order + pl.count;
+    gi.jobs_of = gi.job_start + pl.count + 1;
+    gi.num_problems = pl.count;
+    gi.num_jobs = (int)L.inline_jobs;
+    void* args[] = {&gi, &run};
+    return cudaLaunchKernel(k, dim3(pl.grid), dim3(384), args, te.smem, st);
+  }
+  const GTcEntry& te = kGTc[pl.tc_tile];
+  const void* k = scaled ? te.k1 : te.k0;
+  if (!set_smem_once(k, te.smem, &g_tc_masks[pl.tc_tile][scaled ? 1 : 0]))
+    return cudaErrorInvalidValue;
   void* args[] = {&gt, &run};
   return cudaLaunchKernel(k, dim3(pl.grid), dim3(320), args, te.smem, st);
 }
@@ -416,7 +750,9 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   if (!tile_shape(pl->variant, cfg, &pl->ffma_tile, &pl->tc_tile, &bm, &bn))
     return HBSG_ERR_UNSUPPORTED;
   pl->count = count;
-  pl->L = grouped_layout(count, pr, pl->variant, bm, bn);
+  const GSets sets = grouped_sets(count, pr, pl->variant, cfg);
+  pl->inline_split = sets.any_inline;
+  pl->L = grouped_layout(count, pr, pl->variant, bm, bn, sets);
   const GLayout& L = pl->L;
   if (!ws || ws_bytes < L.total || (reinterpret_cast<uintptr_t>(ws) & 255)) return HBSG_ERR_WORKSPACE;
   pl->ws = static_cast<uint8_t*>(ws);
@@ -463,10 +799,7 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   }
 
   // tile list: problems by K descending (stable), rasterised tiles inside
-  std::vector<int> order(count);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int x, int y) { return pr[x].k > pr[y].k; });
+  const std::vector<int>& order = sets.order;
   const int raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 8;
   std::vector<int4> tiles;
   tiles.reserve(L.num_tiles);
@@ -476,26 +809,29 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
     const int tm = (q.m + bm - 1) / bm, tn = (q.n + bn - 1) / bn;
     for (int g0 = 0; g0 < tm; g0 += raster) {
       const int gm = std::min(raster, tm - g0);
+      const int target = sets.inl[i] ? (int)inline_jobs_of(q) : 0;
       for (int c = 0; c < tn; ++c)
-        for (int r = 0; r < gm; ++r) tiles.push_back(make_int4(i, (g0 + r) * bm, c * bn, 0));
+        for (int r = 0; r < gm; ++r) tiles.push_back(make_int4(i, (g0 + r) * bm, c * bn, target));
     }
   }
 
   std::vector<int4> jobs;
   std::vector<CUtensorMap> maps;
   if (split) {
-    for (int i = 0; i < count; ++i) {  // A split jobs
-      const GProblem& g = probs[i];
-      if (g.M <= 0 || g.N <= 0) continue;
-      const long units = (long)g.M * (g.Kp / 8);
-      for (long u = 0; u < units; u += 2048)
-        jobs.push_back(make_int4(i, (int)u, (int)std::min<long>(2048, units - u), 0));
-    }
-    for (int i = 0; i < count; ++i) {  // B split jobs
-      const GProblem& g = probs[i];
-      if (g.M <= 0 || g.N <= 0) continue;
-      for (int k0 = 0; k0 < g.Kp; k0 += 64)
-        for (int n0 = 0; n0 < g.N; n0 += 64) jobs.push_back(make_int4(i, k0, n0, 0));
+    {
+      for (int i = 0; i < count; ++i) {  // A split jobs (problems split before the product)
+        const GProblem& g = probs[i];
+        if (g.M <= 0 || g.N <= 0 || sets.inl[i]) continue;
+        const long units = (long)g.M * (g.Kp / 8);
+        for (long u = 0; u < units; u += 2048)
+          jobs.push_back(make_int4(i, (int)u, (int)std::min<long>(2048, units - u), 0));
+      }
+      for (int i = 0; i < count; ++i) {  // B split jobs: 64 x 64 blocks
+        const GProblem& g = probs[i];
+        if (g.M <= 0 || g.N <= 0 || sets.inl[i]) continue;
+        for (int k0 = 0; k0 < g.Kp; k0 += 64)
+          for (int n0 = 0; n0 < g.N; n0 += 64) jobs.push_back(make_int4(i, k0, n0, 0));
+      }
     }
     if (scaled) {
       for (int i = 0; i < count; ++i) {
@@ -538,6 +874,28 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   if (e == cudaSuccess && !jobs.empty())
     e = cudaMemcpy(pl->ws + L.jobs_off, jobs.data(), sizeof(int4) * jobs.size(),
                    cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && pl->inline_split) {
+    // order (tile order of the problems), job_start (prefix in that order), jobs_of
+    std::vector<int> tabs(3 * (size_t)count + 1, 0);
+    int* ord = tabs.data();
+    int* jstart = ord + count;
+    int* jof = jstart + count + 1;
+    long acc = 0;
+    for (int i = 0; i < count; ++i) {
+      const int p = order[i];
+      const GProblem& g = probs[p];
+      const long nj = sets.inl[p] ? inline_jobs_of(pr[p]) : 0;
+      (void)g;
+      ord[i] = p;
+      jstart[i] = (int)acc;
+      jof[p] = (int)nj;
+      acc += nj;
+    }
+    jstart[count] = (int)acc;
+    if (acc > 0x7fffffffL) return HBSG_ERR_UNSUPPORTED;
+    e = cudaMemcpy(pl->ws + L.sync_off + L.sync_bytes, tabs.data(), sizeof(int) * tabs.size(),
+                   cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) return status_of(e);
 
   const long slots = split ? sms : (long)sms * (gffma_table(pl->ffma_tile).threads <= 128 ? 2 : 1);
@@ -570,7 +928,8 @@ size_t hbsg_grouped_workspace_size(int count, const hbsg_problem* problems, int 
   if (validate(count, problems, variant) != HBSG_OK) return 0;
   int fi, ti, bm, bn;
   if (!tile_shape(variant, cfg, &fi, &ti, &bm, &bn)) return 0;
-  return grouped_layout(count, problems, variant, bm, bn).total;
+  return grouped_layout(count, problems, variant, bm, bn,
+                        grouped_sets(count, problems, variant, cfg)).total;
 }
 
 int hbsg_grouped_plan_create(hbsg_grouped_plan* out, int count, const hbsg_problem* problems,

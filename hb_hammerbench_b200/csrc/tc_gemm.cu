@@ -47,6 +47,10 @@ struct TcParams {
 // column-major inside a group, so CTAs resident together share operand
 // strips in L2.
 struct SingleTiles {
+  static constexpr bool kInlineSplit = false;
+  __device__ bool wait_ready(int, int, volatile int*, unsigned long long) const { return true; }
+  template <int P, bool SCALED>
+  __device__ void split_worker(int, volatile int*) const {}
   const CUtensorMap* ma;
   const CUtensorMap* mb;
   const TcParams* p;
@@ -63,6 +67,8 @@ struct SingleTiles {
     const int gm = min(p->raster, p->tiles_m - first);
     const int in = t - g * span;
     TileWork w;
+    w.prob = 0;
+    w.ready_target = 0;
     w.ma = ma;
     w.mb = mb;
     w.M = p->M;

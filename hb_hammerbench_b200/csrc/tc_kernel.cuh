@@ -146,7 +146,8 @@ struct TcShape {
   static constexpr int kTmemCols = 2 * BN;  // two accumulator buffers
   static constexpr int kAllocCols = kTmemCols <= 32 ? 32 : kTmemCols <= 64 ? 64 : kTmemCols <= 128 ? 128 : kTmemCols <= 256 ? 256 : 512;
   static constexpr int kBarBytes = 8 * (2 * STAGES + 4) + 16;
-  static constexpr int kSmemBytes = 1024 + STAGES * kStageBytes + kBarBytes;
+  static constexpr int kColExpBytes = 8 * 4 * (BN / 2);  // scaled epilogue: per-warp column exponents
+  static constexpr int kSmemBytes = 1024 + STAGES * kStageBytes + kBarBytes + kColExpBytes;
   static constexpr int kThreads = 320;
   static_assert(kSmemBytes <= 232448, "shared memory");
   static_assert(BN % 16 == 0 && BN >= 64 && BN <= 256, "UMMA N");
@@ -172,6 +173,8 @@ HBSG_DEV float scale_pow2(float x, int s) {
 
 // One output tile of work for the kernel body.
 struct TileWork {
+  int prob;               // problem index (grouped launches; 0 otherwise)
+  int ready_target;       // inline split: jobs that must be done before loading (0 = none)
   const CUtensorMap* ma;  // A parts map (box {32, 128, P})
   const CUtensorMap* mb;  // B parts map (box {32, BN, P})
   float* C;
@@ -193,6 +196,10 @@ struct TcRun {
 
 // Kernel body shared by the single-GEMM and grouped launches. `Tiles` gives
 // count() and get(t); CTA b processes tiles b, b + gridDim.x, ...
+// When Tiles::kInlineSplit is true the CTA has two more warps (10, 11) that
+// produce the BF16 operand parts while the tensor cores work
+// (Tiles::split_worker), and the producer waits for a problem's parts to be
+// complete (Tiles::wait_ready) before loading its first tile.
 template <int P, int BN, int STAGES, bool SCALED, class Tiles>
 __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
   using S = TcShape<P, BN, STAGES>;
@@ -207,6 +214,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
   uint64_t* tempty = bars + 2 * STAGES + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* col_exp = reinterpret_cast<int*>(smem + STAGES * S::kStageBytes + S::kBarBytes);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -242,13 +250,24 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
       uint32_t it = 0;
       bool ok = true;
       const CUtensorMap* last_ma = nullptr;
+      int ready_prob = -1;
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
         const TileWork w = tiles.get(t);
+        if constexpr (Tiles::kInlineSplit) {
+          if (w.ready_target > 0 && w.prob != ready_prob) {
+            if (!tiles.wait_ready(w.prob, w.ready_target, abort_flag, lim)) {
+              ok = false;
+              break;
+            }
+            ready_prob = w.prob;
+          }
+        }
         if (w.ma != last_ma) {
           asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(w.ma)) : "memory");
           asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(w.mb)) : "memory");
           last_ma = w.ma;
         }
+
         for (int kt = 0; kt < w.KT; ++kt, ++it) {
           const int s = it % STAGES;
           const uint32_t ph = (it / STAGES) & 1;
@@ -268,11 +287,15 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      constexpr uint32_t idesc = f16_idesc(kBM, BN);
       uint32_t it = 0, ch = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        const int KT = tiles.get(t).KT;
+        const TileWork w = tiles.get(t);
+        const int KT = w.KT;
+        // MMA width trimmed to the tile's valid columns (multiple of 16): the
+        // last column tile of a problem does no tensor work on padding.
+        const int nv = min(BN, w.N - w.n0);
+        const uint32_t idesc = f16_idesc(kBM, nv >= BN ? BN : ((nv + 15) & ~15));
         const int nchunks = (KT + run.chunk_ktiles - 1) / run.chunk_ktiles;
         int kt = 0;
         for (int c = 0; c < nchunks && ok; ++c, ++ch) {
@@ -310,6 +333,9 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
         }
       }
     }
+  } else if (warp >= 10) {
+    // ---------------- operand splitters (inline-split launches) ----------------
+    if constexpr (Tiles::kInlineSplit) tiles.template split_worker<P, SCALED>(lane, abort_flag);
   } else {
     // ---------------- epilogue (warps 2..9) ----------------
     const int q = warp & 3;         // TMEM lane quadrant this warp may access
@@ -348,6 +374,16 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
       if (!ok) break;
       const int row = w.m0 + 32 * q + lane;
       const int col0 = w.n0 + h * COLS;
+      int* wexp = col_exp + (warp - 2) * COLS;  // this warp's column exponents
+      if constexpr (SCALED) {
+        // each warp stages the exponents of its own COLS columns (no barrier
+        // across warps, so a warp that unwinds early can never strand others)
+        __syncwarp();
+#pragma unroll
+        for (int i = lane; i < COLS; i += 32)
+          wexp[i] = pow2_exp_of_bits(w.colmax[min(col0 + i, w.N - 1)]);
+        __syncwarp();
+      }
       if (row < w.M) {
         float* crow = w.C + (long)row * w.ldc;
         int er = 0;
@@ -359,10 +395,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             float x = sum[j + e];
-            if constexpr (SCALED) {
-              const int cc = min(col0 + j + e, w.N - 1);
-              x = scale_pow2(x, er + pow2_exp_of_bits(w.colmax[cc]));
-            }
+            if constexpr (SCALED) x = scale_pow2(x, er + wexp[j + e]);
             o[e] = x;
           }
           const int c = col0 + j;

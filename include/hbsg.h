@@ -58,6 +58,10 @@ typedef struct hbsg_config {
     int chunk_k;       /* split-BF16: K elements accumulated on the tensor core before the
                           partial is added in FP32 registers (0 = heuristic) */
     int flags;         /* HBSG_FLAG_* */
+    int inline_split_pct; /* grouped split-BF16 plans: percent of the split work (problems
+                             processed last) done by extra warps inside the product kernel
+                             while the tensor cores run; 0 = library default (none),
+                             < 0 = none */
 } hbsg_config;
 
 /* hbsg_config.flags. PRESPLIT_A / PRESPLIT_B: the workspace already holds the
@@ -69,6 +73,7 @@ typedef struct hbsg_config {
 /* SPLIT_ONLY: run only the split passes (fill the workspace), no product;
  * a later call with PRESPLIT_A | PRESPLIT_B computes C from them. */
 #define HBSG_FLAG_SPLIT_ONLY 4
+
 
 typedef struct hbsg_tile_info {
     int variant_class; /* 0 = FFMA kernel family, 1 = split-BF16 tensor-core family */

@@ -1,0 +1,32 @@
+"""Host logic of the benchmark driver (no GPU): case-name parsing in the
+reference's N_<n>__NITER_<k> launch-directory convention and the seeded
+uneven-batch generator."""
+import numpy as np
+import pytest
+
+from hb_hammerbench_b200 import sweep
+
+
+def test_reference_case_name():
+    assert sweep.parse_case("N_512__NITER_2") == {"N": 512, "NITER": 2}
+
+
+def test_general_and_grouped_names():
+    c = sweep.parse_case("M_256__N_256__K_1048576__V_bf16x6__SPLITK_74")
+    assert c == {"M": 256, "N": 256, "K": 1048576, "V": "bf16x6", "SPLITK": 74}
+    g = sweep.parse_case("GROUPED_512__SEED_0__V_ffma")
+    assert g["GROUPED"] == 512 and g["SEED"] == 0
+
+
+@pytest.mark.parametrize("bad", ["N_512__V_fp64", "NITER_2", "N__512", "SEED_1__V_ffma"])
+def test_bad_names(bad):
+    with pytest.raises(ValueError):
+        sweep.parse_case(bad)
+
+
+def test_grouped_dims_distribution():
+    d = sweep.grouped_dims(512, 0)
+    assert d.shape == (512, 3)
+    assert d.min() >= 64 and d.max() <= 2048 and not (d % 32).any()
+    assert np.array_equal(d, sweep.grouped_dims(512, 0))
+    assert not np.array_equal(d, sweep.grouped_dims(512, 1))
