@@ -48,7 +48,8 @@ NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024  # HBSG_NOALLOC_SCRATCH_BYTES
 class TileInfo(ctypes.Structure):
     """struct hbsg_tile_info"""
     _fields_ = [("variant_class", ctypes.c_int), ("bm", ctypes.c_int), ("bn", ctypes.c_int),
-                ("bk", ctypes.c_int), ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_int)]
+                ("bk", ctypes.c_int), ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_int),
+                ("parts", ctypes.c_int)]
 
 
 class SplitLayout(ctypes.Structure):

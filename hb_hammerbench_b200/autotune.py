@@ -1,0 +1,189 @@
+"""Autotuner for the SGEMM schedules (tile shape, K slices, TMEM drain
+interval, rasterisation group) and the grouped plans.
+
+The library's built-in heuristic picks a schedule from the shape alone; the
+tuner measures candidate schedules on the GPU through the C ABI
+(hbsg_gemm_ex / grouped plans with an explicit hbsg_config) and remembers the
+fastest per shape class in a JSON cache, together with every candidate's
+time as evidence. The reference's nearest analogue is its tile-group shape
+sweep (apps/legacy/gemm/sgemm_512/tests.mk:1-6), run by hand.
+
+    from hb_hammerbench_b200 import autotune
+    cfg = autotune.tune(4096, 4096, 4096, "bf16x6")   # measures, caches
+    cfg = autotune.lookup(4000, 4100, 4096, "bf16x6")  # same shape class
+    C = hb.gemm(A, B, variant="bf16x6", config=cfg)
+
+Shape class: the variant and the power-of-two bucket (ceil log2) of M, N
+and K. Cache file: $HBSG_AUTOTUNE_CACHE, else
+~/.cache/hb_hammerbench_b200/autotune.json (written atomically).
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import math
+import os
+import tempfile
+import threading
+
+_lock = threading.Lock()
+_mem: dict | None = None
+
+
+def cache_path() -> str:
+    p = os.environ.get("HBSG_AUTOTUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "hb_hammerbench_b200", "autotune.json")
+
+
+def shape_key(m: int, n: int, k: int, variant: str) -> str:
+    def b(x):
+        return max(0, math.ceil(math.log2(max(1, x))))
+    return f"{variant}:m{b(m)}:n{b(n)}:k{b(k)}"
+
+
+def grouped_key(dims, variant: str) -> str:
+    """Grouped plans: variant, problem count and the bucket of the mean size."""
+    dims = list(dims)
+    mean = sum(m * n * k for m, n, k in dims) / max(1, len(dims))
+    return f"grouped:{variant}:p{len(dims)}:s{round(math.log2(max(1.0, mean)))}"
+
+
+def _load() -> dict:
+    global _mem
+    if _mem is None:
+        try:
+            with open(cache_path()) as f:
+                _mem = json.load(f)
+        except (OSError, ValueError):
+            _mem = {}
+    return _mem
+
+
+def _store(key: str, entry: dict) -> None:
+    with _lock:
+        data = _load()
+        data[key] = entry
+        path = cache_path()
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        fd, tmp = tempfile.mkstemp(dir=os.path.dirname(path) or ".", suffix=".tmp")
+        with os.fdopen(fd, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+
+
+def clear_memory_cache() -> None:
+    global _mem
+    _mem = None
+
+
+def lookup(m: int, n: int, k: int, variant: str) -> dict | None:
+    """Cached best schedule for the shape class, or None."""
+    e = _load().get(shape_key(m, n, k, variant))
+    return dict(e["config"]) if e else None
+
+
+def lookup_grouped(dims, variant: str) -> dict | None:
+    e = _load().get(grouped_key(dims, variant))
+    return dict(e["config"]) if e else None
+
+
+def candidates(m: int, n: int, k: int, variant: str, tiles: list[dict]) -> list[dict]:
+    """Schedules worth measuring for one problem shape."""
+    fam = "ffma" if variant == "ffma" else "bf16"
+    parts = 0 if fam == "ffma" else (3 if "x6" in variant else 2)
+    ids = [t["tile"] for t in tiles if t["family"] == fam and t["parts"] == parts]
+    out = []
+    for tile in ids:
+        t = next(x for x in tiles if x["tile"] == tile)
+        n_tiles = math.ceil(m / t["bm"]) * math.ceil(n / t["bn"])
+        splits = [0]
+        if n_tiles < 148 and k >= 1024:
+            splits = sorted({1, max(1, 148 // n_tiles), max(1, 296 // n_tiles)})
+        if fam == "ffma":
+            splits = [1] + ([s for s in splits if s > 1] if n_tiles < 148 else [])
+        chunks = [0] if fam == "ffma" else ([32, 64] if parts == 3 else [64, 128, 256])
+        rasters = [8, 16] if n_tiles >= 148 else [8]
+        for s, c, r in itertools.product(splits, chunks, rasters):
+            out.append({"tile": tile, "split_k": s, "chunk_k": c, "raster_group": r})
+    return out
+
+
+def _time(fn, steps: int) -> float:
+    import torch
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def tune(m: int, n: int, k: int, variant: str = "bf16x6", steps: int = 5,
+         max_candidates: int = 24, store: bool = True) -> dict:
+    """Measure candidate schedules for an m x n x k product and cache the best.
+
+    FFMA candidates that slice K change the summation order; they are only
+    considered when the output has too few tiles to fill the GPU."""
+    import torch
+
+    from .sgemm import gemm, gemm_workspace_size, tiles
+    g = torch.Generator(device="cuda").manual_seed(1)
+    A = torch.rand((m, k), device="cuda", generator=g) * 2 - 1
+    B = torch.rand((k, n), device="cuda", generator=g) * 2 - 1
+    C = torch.empty((m, n), device="cuda")
+    table = []
+    cands = candidates(m, n, k, variant, tiles())[:max_candidates]
+    for cfg in cands:
+        ws = torch.empty(max(gemm_workspace_size(m, n, k, variant, cfg), 256),
+                         dtype=torch.uint8, device="cuda")
+        try:
+            ms = _time(lambda: gemm(A, B, C, variant=variant, config=cfg, workspace=ws), steps)
+        except Exception as e:  # a schedule the library rejects for this shape
+            table.append({"config": cfg, "error": str(e)})
+            continue
+        table.append({"config": cfg, "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12})
+    ok = [t for t in table if "ms" in t]
+    if not ok:
+        raise RuntimeError("no candidate schedule ran")
+    best = min(ok, key=lambda t: t["ms"])
+    entry = {"config": best["config"], "ms": best["ms"], "shape": [m, n, k],
+             "candidates": table}
+    if store:
+        _store(shape_key(m, n, k, variant), entry)
+    return dict(best["config"])
+
+
+def tune_grouped(As, Bs, variant: str = "bf16x6", steps: int = 3, store: bool = True) -> dict:
+    """Measure grouped-plan schedules (tile shape, rasterisation) on the given
+    problems and cache the best for their class."""
+    from .sgemm import GroupedPlan, tiles
+    fam = "ffma" if variant == "ffma" else "bf16"
+    parts = 0 if fam == "ffma" else (3 if "x6" in variant else 2)
+    ids = [t["tile"] for t in tiles() if t["family"] == fam and t["parts"] == parts]
+    table = []
+    for tile, raster in itertools.product(ids, (8, 16)):
+        cfg = {"tile": tile, "raster_group": raster}
+        try:
+            plan = GroupedPlan(As, Bs, variant=variant, config=cfg)
+            ms = _time(plan.run, steps)
+            plan.close()
+        except Exception as e:
+            table.append({"config": cfg, "error": str(e)})
+            continue
+        table.append({"config": cfg, "ms": ms})
+    ok = [t for t in table if "ms" in t]
+    if not ok:
+        raise RuntimeError("no candidate schedule ran")
+    best = min(ok, key=lambda t: t["ms"])
+    dims = [(a.shape[0], b.shape[1], a.shape[1]) for a, b in zip(As, Bs)]
+    if store:
+        _store(grouped_key(dims, variant), {"config": best["config"], "ms": best["ms"],
+                                            "candidates": table})
+    return dict(best["config"])

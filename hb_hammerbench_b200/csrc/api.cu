@@ -138,7 +138,6 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   if (tile >= total_tiles()) return HBSG_ERR_UNSUPPORTED;
 
   if (variant == HBSG_FFMA) {
-    if (trans_a || trans_b) return HBSG_ERR_UNSUPPORTED;  // FFMA loaders are row-major only
     if (tile >= ffma_num_tiles()) return HBSG_ERR_UNSUPPORTED;
     if (tile < 0) tile = ffma_pick_tile(M, N, K, batch, sms);
     int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
@@ -162,7 +161,7 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
     p.K = K;
     p.splits = splits;
     p.raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 8;
-    return status_from(ffma_launch(tile, p, batch, st));
+    return status_from(ffma_launch(tile, p, batch, st, trans_a ? 1 : 0, trans_b ? 1 : 0));
   }
 
   // ---- split-BF16 on the tensor cores ----

@@ -31,7 +31,12 @@ struct FfmaShape {
 // PAIR selects the packed two-lane FMA (__ffma2_rn, sm_100): each instruction
 // performs two independent IEEE fused multiply-adds, so the per-element
 // arithmetic is unchanged while half as many FMA instructions are issued.
-template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
+// TA / TB: A stored k x m (element (m, k) at A[k*lda + m]) / B stored n x k
+// (element (k, n) at B[n*ldb + k]). Transposed operands use the 4-byte copy
+// path with the thread order chosen for coalesced global reads; the shared
+// memory layouts, and so the arithmetic, are the same as for row-major.
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR,
+          bool TA = false, bool TB = false>
 __device__ __forceinline__ void ffma_tile(const float* __restrict__ A, long lda,
                                           const float* __restrict__ B, long ldb, int M, int N,
                                           int k_begin, int k_end, int m0, int n0, float* C,
@@ -90,23 +95,26 @@ __device__ __forceinline__ void ffma_tile(const float* __restrict__ A, long lda,
         cp_async16(bs + r * BN + nc, src, bytes);
       }
     } else {
+      static_assert(!(VEC && (TA || TB)), "transposed operands use the 4-byte path");
 #pragma unroll 4
       for (int c = tid; c < BM * BK; c += NT) {
-        const int r = c / BK;
-        const int kc = c % BK;
+        const int r = TA ? c % BM : c / BK;   // transposed: m fastest (contiguous)
+        const int kc = TA ? c / BM : c % BK;  // row-major: k fastest (contiguous)
         const int gr = m0 + r;
         const int gk = k0 + kc;
         const bool ok = gr < M && gk < k_end;
-        cp_async4(as + r * AS + kc, ok ? A + (long)gr * lda + gk : A, ok ? 4 : 0);
+        const long off = TA ? (long)gk * lda + gr : (long)gr * lda + gk;
+        cp_async4(as + r * AS + kc, ok ? A + off : A, ok ? 4 : 0);
       }
 #pragma unroll 4
       for (int c = tid; c < BK * BN; c += NT) {
-        const int r = c / BN;
-        const int nc = c % BN;
+        const int r = c / BN;  // n fastest: conflict-free shared stores; for a
+        const int nc = c % BN; // transposed B the row reads are absorbed by L1
         const int gk = k0 + r;
         const int gn = n0 + nc;
         const bool ok = gk < k_end && gn < N;
-        cp_async4(bs + r * BN + nc, ok ? B + (long)gk * ldb + gn : B, ok ? 4 : 0);
+        const long off = TB ? (long)gn * ldb + gk : (long)gk * ldb + gn;
+        cp_async4(bs + r * BN + nc, ok ? B + off : B, ok ? 4 : 0);
       }
     }
   };

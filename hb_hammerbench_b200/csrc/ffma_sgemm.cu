@@ -25,7 +25,8 @@
 
 namespace hbsg {
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR,
+          bool TA = false, bool TB = false>
 __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
     ffma_sgemm_kernel(FfmaParams p) {
   extern __shared__ __align__(16) float smem[];
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThread
     ldc = p.ldc;
     vec_store = p.vec_store;
   }
-  ffma_tile<BM, BN, BK, WM, WN, STAGES, VEC, PAIR>(p.A + batch * p.strideA, p.lda,
+  ffma_tile<BM, BN, BK, WM, WN, STAGES, VEC, PAIR, TA, TB>(p.A + batch * p.strideA, p.lda,
                                                    p.B + batch * p.strideB, p.ldb, p.M, p.N,
                                                    k_begin, k_end, m0, n0, C, ldc, vec_store, smem);
 }
@@ -100,6 +101,23 @@ static cudaError_t launch_ffma(const FfmaParams& p, dim3 grid, cudaStream_t st, 
   return cudaGetLastError();
 }
 
+// Transposed-operand kernels (4-byte copy path) for a tile shape.
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+static cudaError_t launch_ffma_trans(const FfmaParams& p, dim3 grid, cudaStream_t st, int ta,
+                                     int tb) {
+  using S = FfmaShape<BM, BN, BK, WM, WN, STAGES>;
+  auto k10 = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, true, true, false>;
+  auto k01 = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, true, false, true>;
+  auto k11 = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, true, true, true>;
+  auto k = ta && tb ? k11 : ta ? k10 : k01;
+  static uint32_t masks[3] = {0, 0, 0};
+  const int slot = ta && tb ? 2 : ta ? 0 : 1;
+  if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, &masks[slot]))
+    return cudaErrorInvalidValue;
+  k<<<grid, S::kThreads, S::kSmemBytes, st>>>(p);
+  return cudaGetLastError();
+}
+
 #define HBSG_FFMA_ENTRY(BM, BN, BK, WM, WN, ST, PAIR)                                   \
   FfmaEntry {                                                                           \
     BM, BN, BK, WM, WN, ST, FfmaShape<BM, BN, BK, WM, WN, ST>::kThreads,                \
@@ -131,6 +149,7 @@ bool ffma_tile_info(int idx, hbsg_tile_info* out) {
   out->bk = e.bk;
   out->threads = e.threads;
   out->smem_bytes = e.smem;
+  out->parts = 0;
   return true;
 }
 
@@ -165,7 +184,13 @@ size_t ffma_workspace_bytes(int M, int N, int batch, int splits) {
   return splits > 1 ? (size_t)M * N * batch * splits * sizeof(float) : 0;
 }
 
-cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st) {
+cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st, int ta, int tb) {
+  // transposed operands: 128 x 128 or 64 x 64 tiles (the closest of the two)
+  if (ta || tb) {
+    const FfmaEntry& big = kFfmaTiles[0];
+    const FfmaEntry& e0 = kFfmaTiles[tile_idx];
+    tile_idx = (e0.bm * e0.bn >= big.bm * big.bn) ? 0 : 2;
+  }
   const FfmaEntry& e = kFfmaTiles[tile_idx];
   p.tiles_m = (p.M + e.bm - 1) / e.bm;
   p.tiles_n = (p.N + e.bn - 1) / e.bn;
@@ -180,14 +205,20 @@ cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st) 
   } else {
     p.k_per_split = p.K;
   }
-  const bool vec = ((p.lda & 3) == 0) && ((p.ldb & 3) == 0) &&
+  const bool vec = !ta && !tb && ((p.lda & 3) == 0) && ((p.ldb & 3) == 0) &&
                    ((reinterpret_cast<uintptr_t>(p.A) & 15) == 0) &&
                    ((reinterpret_cast<uintptr_t>(p.B) & 15) == 0) && ((p.strideA & 3) == 0) &&
                    ((p.strideB & 3) == 0);
   p.vec_store = ((p.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
                 ((p.strideC & 3) == 0);
   dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)p.splits, (unsigned)batch);
-  cudaError_t err = e.launch(p, grid, st, vec);
+  cudaError_t err;
+  if (ta || tb) {
+    err = tile_idx == 0 ? launch_ffma_trans<128, 128, 16, 64, 64, 4>(p, grid, st, ta, tb)
+                        : launch_ffma_trans<64, 64, 16, 32, 32, 4>(p, grid, st, ta, tb);
+  } else {
+    err = e.launch(p, grid, st, vec);
+  }
   if (err != cudaSuccess || p.splits == 1) return err;
   return splitk_reduce(p.partial, p.C, p.M, p.N, p.ldc, p.strideC, p.splits, batch, 148, st);
 }

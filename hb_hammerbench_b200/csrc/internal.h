@@ -29,7 +29,8 @@ int ffma_num_tiles();
 bool ffma_tile_info(int idx, hbsg_tile_info* out);
 int ffma_pick_tile(int M, int N, int K, int batch, int num_sms);
 size_t ffma_workspace_bytes(int M, int N, int batch, int splits);
-cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st);
+cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st, int ta = 0,
+                        int tb = 0);
 
 // ---- split-BF16 family ----------------------------------------------------------
 cudaError_t split_operand_a(const float* A, long lda, int M, int K, int Kp, int parts, bool scaled,

@@ -181,6 +181,7 @@ bool tc_tile_info(int idx, hbsg_tile_info* out) {
   out->bk = kBK;
   out->threads = 320;
   out->smem_bytes = e.smem;
+  out->parts = e.parts;
   return true;
 }
 

@@ -217,7 +217,8 @@ def tiles() -> list[dict]:
         check(lib().hbsg_tile_describe(t, ctypes.byref(info)), "hbsg_tile_describe")
         out.append({"tile": t, "family": "ffma" if info.variant_class == 0 else "bf16",
                     "bm": info.bm, "bn": info.bn, "bk": info.bk,
-                    "threads": info.threads, "smem_bytes": info.smem_bytes})
+                    "threads": info.threads, "smem_bytes": info.smem_bytes,
+                    "parts": info.parts})
     return out
 
 

@@ -80,6 +80,8 @@ typedef struct hbsg_tile_info {
     int bm, bn, bk;    /* CTA tile */
     int threads;       /* threads per CTA */
     int smem_bytes;    /* dynamic shared memory per CTA */
+    int parts;         /* split-BF16 family: BF16 parts per operand (3 -> BF16X6 forms,
+                          2 -> BF16X3 forms); 0 for the FFMA family */
 } hbsg_tile_info;
 
 /* ---------------------------------------------------------------------------

@@ -156,3 +156,15 @@ def test_stream_ordering(hb, oracle_mod):
     s.synchronize()
     exp = oracle_mod.host_mm_fma(oracle_mod.host_mm_fma(A, B), B)
     assert np.array_equal(c2.cpu().numpy(), exp)
+
+
+@pytest.mark.parametrize("ta,tb", [(1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("m,n,k", [(300, 200, 130), (1000, 1024, 512), (33, 65, 17)])
+def test_transposed_operands_bit_exact(hb, oracle_mod, ta, tb, m, n, k):
+    # the legacy data-parallel kernel's transposed-A load
+    # (apps/legacy/gemm/sgemm_data_parallel/kernel.cpp:21-48), both operands here
+    A, B = oracle_mod.uniform_inputs((m, k), (k, n), seed=m + 7 * n + 13 * k + ta + 2 * tb)
+    a = _dev(np.ascontiguousarray(A.T)) if ta else _dev(A)
+    b = _dev(np.ascontiguousarray(B.T)) if tb else _dev(B)
+    out = hb.gemm(a, b, trans_a=bool(ta), trans_b=bool(tb)).cpu().numpy()
+    assert np.array_equal(out, oracle_mod.host_mm_fma(A, B))
