@@ -68,7 +68,9 @@ def _profile_traffic(name: str):
 # clocks during the timed region
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi samples every 100 ms; only samples taken inside the marked
+    timed windows are summarised."""
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -76,6 +78,12 @@ class ClockSampler:
         self.gpu_index = gpu_index
         self.proc = None
         self.path = None
+        self.windows = []
+
+    def window(self, t0: float, t1: float):
+        import datetime
+        self.windows.append((datetime.datetime.fromtimestamp(t0),
+                             datetime.datetime.fromtimestamp(t1)))
 
     def start(self):
         try:
@@ -97,11 +105,18 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        import datetime
         sm, mx, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
+                continue
+            try:
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+            except ValueError:
+                continue
+            if self.windows and not any(a <= ts <= b for a, b in self.windows):
                 continue
             try:
                 sm.append(float(f[1]))
@@ -224,6 +239,8 @@ def run_ours(args) -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
+    sampler = ClockSampler(local)  # summarises the samples inside the timed windows
+
     def timed(step_fn, steps, per_step=True):
         """K steps on `stream`; returns (total ms max over ranks, per-step kernel ms)."""
         for _ in range(warmup):
@@ -234,11 +251,13 @@ def run_ours(args) -> None:
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         barrier()
+        w0 = time.time()
         t0.record(stream)
         for i in range(steps):
             step_fn(evs[i] if per_step else None)
         t1.record(stream)
         barrier()
+        sampler.window(w0, time.time())
         total = torch.tensor([t0.elapsed_time(t1)], device=dev)
         if ws > 1:
             dist.all_reduce(total, op=dist.ReduceOp.MAX)
@@ -259,15 +278,14 @@ def run_ours(args) -> None:
             if ev:
                 ev[1].record(stream)
 
-    sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
     total_ms, kern_ms = timed(step_main, args.steps)
-    clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
     value = ws * flops * args.steps / (total_ms * 1e-3) / 1e12
 
     if args.profile:
+        sampler.stop()
         if rank == 0:
             print(json.dumps({"profile_run": True, "variant": variant, "ms_per_step": ms_per_step}),
                   flush=True)
@@ -310,6 +328,7 @@ def run_ours(args) -> None:
         hb.gemm(dA, dB, C, variant=variant, workspace=wsp)
         hC.copy_(C, non_blocking=True)
     e_total, _ = timed(step_e2e, args.steps, per_step=False)
+    clocks = sampler.stop()
     e2e_val = ws * flops * args.steps / (e_total * 1e-3) / 1e12
     assert torch.equal(hC, C.cpu())
 
@@ -374,7 +393,7 @@ def run_ours(args) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default="bf16x6",
