@@ -164,6 +164,22 @@ def cpu_baseline(n: int, seconds: float = 12.0, threads: int = 0) -> dict:
 
 # ---------------------------------------------------------------------------
 
+def replica_throughput(local_ms: float, flops_per_step: float, steps: int,
+                       world: int = 1, device=None) -> tuple[float, float]:
+    """Whole-job throughput of `world` replicas that each ran `steps` steps of
+    `flops_per_step`: the job time is the maximum of the ranks' device times
+    (an all-reduce over the default process group when world > 1). Returns
+    (max time in ms, TFLOP/s summed over ranks)."""
+    t = local_ms
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        x = torch.tensor([local_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        t = float(x.item())
+    return t, world * flops_per_step * steps / (t * 1e-3) / 1e12
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -258,10 +274,8 @@ def run_ours(args) -> None:
         t1.record(stream)
         barrier()
         sampler.window(w0, time.time())
-        total = torch.tensor([t0.elapsed_time(t1)], device=dev)
-        if ws > 1:
-            dist.all_reduce(total, op=dist.ReduceOp.MAX)
-        return float(total.item()), ([a.elapsed_time(b) for a, b in evs] if per_step else [])
+        total, _ = replica_throughput(t0.elapsed_time(t1), flops, steps, ws, dev)
+        return total, ([a.elapsed_time(b) for a, b in evs] if per_step else [])
 
     def step_main(ev):
         if split:
@@ -282,7 +296,7 @@ def run_ours(args) -> None:
     time.sleep(0.3)
     total_ms, kern_ms = timed(step_main, args.steps)
     ms_per_step = total_ms / args.steps
-    value = ws * flops * args.steps / (total_ms * 1e-3) / 1e12
+    value = ws * flops * args.steps / (total_ms * 1e-3) / 1e12  # total_ms: max over ranks
 
     if args.profile:
         sampler.stop()
