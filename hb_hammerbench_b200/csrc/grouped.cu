@@ -578,10 +578,11 @@ static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* 
   int idx = -1;
   if (tile >= 0) {
     idx = tile - nf;
-    if (idx < 0 || idx >= tc_num_tiles() || tc_tile_parts(idx) != P) return false;
+    if (idx < 0 || idx >= tc_num_tiles() || tc_tile_parts(idx) != P || tc_tile_pair(idx))
+      return false;  // grouped plans run the single-CTA tiles
   } else {
-    for (int i = 0; i < tc_num_tiles(); ++i)  // default: the BN = 256 tile
-      if (tc_tile_parts(i) == P && tc_tile_bn(i) == 256) idx = i;
+    for (int i = 0; i < tc_num_tiles(); ++i)  // default: the single-CTA BN = 256 tile
+      if (tc_tile_parts(i) == P && tc_tile_bn(i) == 256 && !tc_tile_pair(i)) idx = i;
   }
   if (idx < 0) return false;
   tc_tile_info(idx, &info);
@@ -858,6 +859,7 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
         return HBSG_ERR_UNSUPPORTED;
     }
     pl->run.chunk_ktiles = tc_chunk_ktiles(P, cfg ? cfg->chunk_k : 0);
+    pl->run.l2_ahead = tc_l2_ahead();
     pl->run.wait_limit_ns = kWaitLimitNs;
     pl->run.debug_skip_loads = 0;
   }

@@ -26,8 +26,9 @@
 // Every wait is bounded: after kWaitLimitNs the kernel records
 // HBSG_ERR_DEVICE_TIMEOUT in the device error flag and unwinds.
 #include <algorithm>
+#include <cstdlib>
 
-#include "tc_kernel.cuh"
+#include "tc_kernel2.cuh"
 
 namespace hbsg {
 
@@ -57,7 +58,7 @@ struct SingleTiles {
   // Work item t = slice * num_tiles + tile: with split-K the slices of all
   // tiles are independent items; slice s covers k-tiles [s*kts, (s+1)*kts)
   // and writes its partial to C + s*M*N (row stride N).
-  template <int BN>
+  template <int TBM, int BN>
   __device__ __forceinline__ TileWork get_bn(int item) const {
     const int slice = item / p->num_tiles;
     const int t = item - slice * p->num_tiles;
@@ -73,7 +74,7 @@ struct SingleTiles {
     w.mb = mb;
     w.M = p->M;
     w.N = p->N;
-    w.m0 = (first + in % gm) * kBM;
+    w.m0 = (first + in % gm) * TBM;
     w.n0 = (in / gm) * BN;
     const int KT = p->Kp / kBK;
     w.kt0 = slice * p->kt_per_split;
@@ -91,10 +92,10 @@ struct SingleTiles {
   }
 };
 
-template <int BN>
+template <int BN, int TBM = kBM>
 struct SingleTilesBN : SingleTiles {
   __device__ __forceinline__ int count() const { return p->num_tiles * p->splits; }
-  __device__ __forceinline__ TileWork get(int t) const { return get_bn<BN>(t); }
+  __device__ __forceinline__ TileWork get(int t) const { return get_bn<TBM, BN>(t); }
 };
 
 template <int P, int BN, int STAGES, bool SCALED>
@@ -106,6 +107,18 @@ __global__ void __launch_bounds__(320, 1)
   tiles.mb = &tmB;
   tiles.p = &p;
   tc_body<P, BN, STAGES, SCALED>(tiles, run);
+}
+
+// CTA-pair form: 256 x BN tiles on a cluster of two CTAs (tc_kernel2.cuh).
+template <int P, int BN, int STAGES, bool SCALED>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(320, 1)
+    tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ TcParams p, const TcRun run) {
+  SingleTilesBN<BN, 2 * kBM> tiles;
+  tiles.ma = &tmA;
+  tiles.mb = &tmB;
+  tiles.p = &p;
+  tc_pair_body<P, BN, STAGES, SCALED>(tiles, run);
 }
 
 // ---------------------------------------------------------------------------
@@ -143,6 +156,7 @@ bool tc_make_parts_map_impl(CUtensorMap* map, const void* parts, int P, int rows
 
 struct TcEntry {
   int parts, bn, stages;
+  int pair;  // 1: CTA-pair kernel, 256-row tiles
   int smem;
   cudaError_t (*launch)(const CUtensorMap&, const CUtensorMap&, const TcParams&, const TcRun&,
                         int grid, cudaStream_t, bool scaled);
@@ -163,11 +177,29 @@ static cudaError_t launch_tc(const CUtensorMap& a, const CUtensorMap& b, const T
 }
 
 #define HBSG_TC_ENTRY(P, BN, ST) \
-  TcEntry { P, BN, ST, TcShape<P, BN, ST>::kSmemBytes, &launch_tc<P, BN, ST> }
+  TcEntry { P, BN, ST, 0, TcShape<P, BN, ST>::kSmemBytes, &launch_tc<P, BN, ST> }
 
 // Ordered by parts: entries with parts == 3 serve BF16X6, parts == 2 BF16X3.
+template <int P, int BN, int STAGES>
+static cudaError_t launch_tc_pair(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p,
+                                  const TcRun& run, int grid, cudaStream_t st, bool scaled) {
+  using S = TcPairShape<P, BN, STAGES>;
+  auto k0 = tc_pair_kernel<P, BN, STAGES, false>;
+  auto k1 = tc_pair_kernel<P, BN, STAGES, true>;
+  auto k = scaled ? k1 : k0;
+  static uint32_t m0 = 0, m1 = 0;
+  if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, scaled ? &m1 : &m0))
+    return cudaErrorInvalidValue;
+  k<<<grid, 320, S::kSmemBytes, st>>>(a, b, p, run);
+  return cudaGetLastError();
+}
+#define HBSG_TC_PAIR_ENTRY(P, BN, ST) \
+  TcEntry { P, BN, ST, 1, TcPairShape<P, BN, ST>::kSmemBytes, &launch_tc_pair<P, BN, ST> }
+
 #define HBSG_TC_ENTRY_COMMA(P, BN, ST) HBSG_TC_ENTRY(P, BN, ST),
-static const TcEntry kTcTiles[] = {HBSG_TC_TILE_LIST(HBSG_TC_ENTRY_COMMA)};
+static const TcEntry kTcTiles[] = {HBSG_TC_TILE_LIST(HBSG_TC_ENTRY_COMMA)
+                                   HBSG_TC_PAIR_ENTRY(3, 256, 4),   // 256 x 256 pair, 6 products
+                                   HBSG_TC_PAIR_ENTRY(2, 256, 6)};  // 256 x 256 pair, 3 products
 static constexpr int kNumTcTiles = sizeof(kTcTiles) / sizeof(kTcTiles[0]);
 
 int tc_num_tiles() { return kNumTcTiles; }
@@ -176,7 +208,7 @@ bool tc_tile_info(int idx, hbsg_tile_info* out) {
   if (idx < 0 || idx >= kNumTcTiles) return false;
   const TcEntry& e = kTcTiles[idx];
   out->variant_class = 1;
-  out->bm = kBM;
+  out->bm = e.pair ? 2 * kBM : kBM;
   out->bn = e.bn;
   out->bk = kBK;
   out->threads = 320;
@@ -187,6 +219,32 @@ bool tc_tile_info(int idx, hbsg_tile_info* out) {
 
 int tc_tile_parts(int idx) { return kTcTiles[idx].parts; }
 int tc_tile_bn(int idx) { return kTcTiles[idx].bn; }
+int tc_tile_pair(int idx) { return kTcTiles[idx].pair; }
+
+// Co-resident clusters of two CTAs for a pair kernel (0 if unknown).
+template <int P, int BN, int STAGES>
+static int pair_clusters(bool scaled) {
+  using S = TcPairShape<P, BN, STAGES>;
+  const void* k = scaled ? reinterpret_cast<const void*>(&tc_pair_kernel<P, BN, STAGES, true>)
+                         : reinterpret_cast<const void*>(&tc_pair_kernel<P, BN, STAGES, false>);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(320, 1, 1);
+  cfg.dynamicSmemBytes = S::kSmemBytes;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = 2;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
 
 bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, int box_rows) {
   return tc_make_parts_map_impl(static_cast<CUtensorMap*>(map), parts, P, rows, Kp, box_rows);
@@ -198,10 +256,12 @@ int tc_pick_tile(int M, int N, int parts, int sms) {
   for (int i = 0; i < kNumTcTiles; ++i) {
     const TcEntry& e = kTcTiles[i];
     if (e.parts != parts) continue;
-    const long tiles = (long)((M + kBM - 1) / kBM) * ((N + e.bn - 1) / e.bn);
-    const double waves = (double)tiles / sms;
+    const int tbm = e.pair ? 2 * kBM : kBM;
+    const long tiles = (long)((M + tbm - 1) / tbm) * ((N + e.bn - 1) / e.bn);
+    const double waves = (double)tiles / (e.pair ? sms / 2 : sms);
     const double eff = waves / ceil(waves);
-    const double width = e.bn == 256 ? 1.0 : e.bn == 128 ? 0.85 : 0.6;  // smem bytes per MMA
+    // shared-memory operand bytes per MMA flop (the single-CTA bound)
+    const double width = e.pair ? 0.9 : e.bn == 256 ? 0.95 : e.bn == 128 ? 0.8 : 0.55;
     const double waste = (double)N / (((N + e.bn - 1) / e.bn) * e.bn);
     const double score = eff * width * waste * fmin(1.0, waves);
     if (score > best_score + 1e-9) {
@@ -219,11 +279,13 @@ int tc_pick_tile(int M, int N, int parts, int sms) {
 int tc_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
   const TcEntry& e = kTcTiles[idx];
   const int KT = ((K + 31) / 32 * 32) / kBK > 0 ? ((K + 31) / 32 * 32) / kBK : 1;
-  const long tiles = (long)((M + kBM - 1) / kBM) * ((N + e.bn - 1) / e.bn);
+  const int tbm = e.pair ? 2 * kBM : kBM;
+  const long tiles = (long)((M + tbm - 1) / tbm) * ((N + e.bn - 1) / e.bn);
+  const int slots = e.pair ? sms / 2 : sms;  // concurrent work items
   int s = requested;
   if (s <= 0) {
     s = 1;
-    if (tiles * 2 <= sms) s = (int)std::min<long>((sms + tiles - 1) / tiles, std::max(1, KT / 8));
+    if (tiles * 2 <= slots) s = (int)std::min<long>((slots + tiles - 1) / tiles, std::max(1, KT / 8));
   }
   s = std::max(1, std::min(s, KT));
   int per = (KT + s - 1) / s;
@@ -240,13 +302,15 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
   const TcEntry& e = kTcTiles[idx];
   CUtensorMap ma, mb;
   if (!tc_make_parts_map_impl(&ma, Ap, e.parts, M, Kp, kBM)) return cudaErrorInvalidValue;
-  if (!tc_make_parts_map_impl(&mb, Bp, e.parts, N, Kp, e.bn)) return cudaErrorInvalidValue;
+  if (!tc_make_parts_map_impl(&mb, Bp, e.parts, N, Kp, e.pair ? e.bn / 2 : e.bn))
+    return cudaErrorInvalidValue;
   TcParams p{};
   p.M = M;
   p.N = N;
   p.K = K;
   p.Kp = Kp;
-  p.tiles_m = (M + kBM - 1) / kBM;
+  const int tbm = e.pair ? 2 * kBM : kBM;
+  p.tiles_m = (M + tbm - 1) / tbm;
   p.tiles_n = (N + e.bn - 1) / e.bn;
   p.num_tiles = p.tiles_m * p.tiles_n;
   p.raster = raster > 0 ? raster : 16;
@@ -259,21 +323,48 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
   p.colmax = colmax;
   TcRun run;
   run.chunk_ktiles = tc_chunk_ktiles(e.parts, chunk_k);
+  run.l2_ahead = tc_l2_ahead();
   run.debug_skip_loads = debug_skip_loads;
   run.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;
   const long items = (long)p.num_tiles * p.splits;
-  const int grid = (int)(items < sms ? items : sms);
+  int grid;
+  if (e.pair) {
+    // every pair must be resident at once (tiles are dealt statically)
+    int resident = e.parts == 3 ? pair_clusters<3, 256, 4>(rowmax != nullptr)
+                                : pair_clusters<2, 256, 6>(rowmax != nullptr);
+    if (resident <= 0) resident = sms / 2;
+    const long cap = std::min<long>(resident, sms / 2);
+    const long pairs = items < cap ? items : cap;
+    grid = (int)(2 * pairs);
+  } else {
+    grid = (int)(items < sms ? items : sms);
+  }
   cudaError_t err = e.launch(ma, mb, p, run, grid, st, rowmax != nullptr);
   if (err != cudaSuccess || p.splits == 1) return err;
   return splitk_reduce(partial, C, M, N, ldc, 0, p.splits, 1, sms, st);
 }
 
-// Default drain interval: every k-tile for the 6-product form (its error is
-// dominated by tensor-core accumulation, and draining is free at this rate),
-// every 4 k-tiles for the 3-product form (dominated by the 2-part split).
+// Default drain interval: every 2 k-tiles (64 of K) for the 6-product form,
+// every 4 k-tiles for the 3-product form. Measured at 8192^3 (6-product):
+// interval 32 / 64 / 128 / 256 of K gave 4.63 / 4.38 / 4.11 / 4.03 ms and
+// relative error 3.4e-7 / 4.4e-7 / 8.2e-7 / 1.6e-6 against FP64 (FFMA:
+// 1.6e-6); 64 keeps the error 3.7x below FFMA's. The 3-product form's error
+// is set by its 2-part split, not by the interval.
 int tc_chunk_ktiles(int parts, int chunk_k) {
-  const int ck = chunk_k > 0 ? chunk_k : (parts == 3 ? 32 : 128);
+  const int ck = chunk_k > 0 ? chunk_k : (parts == 3 ? 64 : 128);
   return ck / kBK > 0 ? ck / kBK : 1;
+}
+
+// k-tiles the producer prefetches into L2 ahead of its loads
+// (HBSG_TC_L2_AHEAD overrides the default, for tuning).
+int tc_l2_ahead() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("HBSG_TC_L2_AHEAD");
+    v = e ? atoi(e) : 0;  // off: measured slower at 2, 4 and 8 (extra TMA operations)
+    if (v < 0) v = 0;
+  }
+  return v;
 }
 
 int tc_read_and_clear_device_error() {

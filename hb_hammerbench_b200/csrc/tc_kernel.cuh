@@ -65,6 +65,15 @@ HBSG_DEV void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, 
       : "memory");
 }
 
+// L2 prefetch of one 3-D tensor box (no shared-memory destination, no
+// completion): keeps operand tiles warm in L2 ahead of the smem ring.
+HBSG_DEV void tma_prefetch_3d(const CUtensorMap* map, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+
 HBSG_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 HBSG_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
@@ -190,6 +199,7 @@ struct TileWork {
 // Settings shared by every tile of a launch.
 struct TcRun {
   int chunk_ktiles;                  // k-tiles accumulated in TMEM before draining
+  int l2_ahead;                      // k-tiles prefetched into L2 ahead of the loads (0 = off)
   unsigned long long wait_limit_ns;  // bound of every mbarrier wait
   int debug_skip_loads;              // test hook: producer never loads (forces the timeout path)
 };
@@ -251,8 +261,14 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
       bool ok = true;
       const CUtensorMap* last_ma = nullptr;
       int ready_prob = -1;
+      TileWork w;
+      if (blockIdx.x < num_tiles) w = tiles.get(blockIdx.x);
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        const TileWork w = tiles.get(t);
+        // the next tile's description is fetched one tile ahead, so its
+        // global loads never sit on the critical path at a tile switch
+        TileWork nx = w;
+        const bool has_next = t + (int)gridDim.x < num_tiles;
+        if (has_next) nx = tiles.get(t + gridDim.x);
         if constexpr (Tiles::kInlineSplit) {
           if (w.ready_target > 0 && w.prob != ready_prob) {
             if (!tiles.wait_ready(w.prob, w.ready_target, abort_flag, lim)) {
@@ -267,7 +283,6 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(w.mb)) : "memory");
           last_ma = w.ma;
         }
-
         for (int kt = 0; kt < w.KT; ++kt, ++it) {
           const int s = it % STAGES;
           const uint32_t ph = (it / STAGES) & 1;
@@ -281,7 +296,25 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           mbar_arrive_expect_tx(&full[s], S::kStageBytes);
           tma_load_3d(sa, w.ma, (w.kt0 + kt) * kBK, w.m0, 0, &full[s]);
           tma_load_3d(sb, w.mb, (w.kt0 + kt) * kBK, w.n0, 0, &full[s]);
+          if (run.l2_ahead > 0) {  // the k-tile l2_ahead steps further, possibly of the next tile
+            const int ka = kt + (kt == 0 ? 1 : run.l2_ahead);
+            const int kend = kt == 0 ? min(w.KT, 1 + run.l2_ahead) : ka + 1;
+            for (int kp = ka; kp < kend; ++kp) {  // at kt == 0: warm the whole lookahead window
+              if (kp < w.KT) {
+                tma_prefetch_3d(w.ma, (w.kt0 + kp) * kBK, w.m0, 0);
+                tma_prefetch_3d(w.mb, (w.kt0 + kp) * kBK, w.n0, 0);
+              } else if (has_next && kp - w.KT < nx.KT) {
+                tma_prefetch_3d(nx.ma, (nx.kt0 + kp - w.KT) * kBK, nx.m0, 0);
+                tma_prefetch_3d(nx.mb, (nx.kt0 + kp - w.KT) * kBK, nx.n0, 0);
+              }
+            }
+          }
+          if (kt == 0 && has_next && nx.ma != w.ma) {  // warm the next problem's maps
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(nx.ma)) : "memory");
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(nx.mb)) : "memory");
+          }
         }
+        w = nx;
       }
     }
   } else if (warp == 1) {
@@ -289,8 +322,11 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
     if (lane == 0) {
       uint32_t it = 0, ch = 0;
       bool ok = true;
+      TileWork w;
+      if (blockIdx.x < num_tiles) w = tiles.get(blockIdx.x);
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        const TileWork w = tiles.get(t);
+        TileWork nx = w;  // fetched one tile ahead (see the producer)
+        if (t + (int)gridDim.x < num_tiles) nx = tiles.get(t + gridDim.x);
         const int KT = w.KT;
         // MMA width trimmed to the tile's valid columns (multiple of 16): the
         // last column tile of a problem does no tensor work on padding.
@@ -331,6 +367,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           }
           if (ok) tc_commit(&tfull[buf]);
         }
+        w = nx;
       }
     }
   } else if (warp >= 10) {

@@ -14,7 +14,8 @@ KEY_value fields. Recognised keys:
                              run as one grouped plan (CUDA-graph replay)
   V_<variant>                ffma | bf16x3 | bf16x6 | bf16x3_scaled | bf16x6_scaled
   DIST_<d>                   uniform (U[-1,1), default) | wide (sign * 2^u, u ~ U[-20,20])
-  SPLITK_<s> / TILE_<t>      explicit schedule (hbsg_config.split_k / .tile)
+  SPLITK_<s> / TILE_<t> / CHUNK_<c>
+                             explicit schedule (hbsg_config.split_k / .tile / .chunk_k)
 
 Examples: N_512__NITER_2, N_8192__NITER_1__V_bf16x6, M_256__N_256__K_1048576__V_bf16x6,
 GROUPED_512__SEED_0__V_bf16x6, N_8192__NITER_1__V_bf16x6_scaled__DIST_wide.
@@ -85,6 +86,8 @@ def _config(c: dict):
         cfg["split_k"] = c["SPLITK"]
     if "TILE" in c:
         cfg["tile"] = c["TILE"]
+    if "CHUNK" in c:
+        cfg["chunk_k"] = c["CHUNK"]
     return cfg or None
 
 

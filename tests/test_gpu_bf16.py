@@ -259,3 +259,21 @@ def test_split_k_workspace_reported(hb):
     need_auto = hb.gemm_workspace_size(m, n, k, "bf16x6")
     need_one = hb.gemm_workspace_size(m, n, k, "bf16x6", config={"split_k": 1})
     assert need_auto > need_one  # the heuristic splits this shape (2 tiles)
+
+
+@pytest.mark.parametrize("variant,pair_tile,single_tile", [("bf16x6", 16, 10), ("bf16x3", 17, 13)])
+@pytest.mark.parametrize("m,n,k", [(256, 256, 64), (1000, 700, 300), (2048, 1536, 1024)])
+def test_cta_pair_tiles_match_single_cta(hb, variant, pair_tile, single_tile, m, n, k):
+    # the CTA-pair kernel (tcgen05 cta_group::2, 256-row tiles) issues the same
+    # products in the same order per output element as the single-CTA kernel
+    import torch
+    A = _rand((m, k), m + 3 * k)
+    B = _rand((k, n), n + 5 * k)
+    cfg = {"split_k": 1, "chunk_k": 64}
+    C2 = hb.gemm(A, B, variant=variant, config={**cfg, "tile": pair_tile})
+    C1 = hb.gemm(A, B, variant=variant, config={**cfg, "tile": single_tile})
+    assert torch.equal(C1, C2)
+    # and with K slices
+    C3 = hb.gemm(A, B, variant=variant, config={"split_k": 3, "tile": pair_tile})
+    ref = A.double() @ B.double()
+    assert _err(C3, ref)[0] < (2.0 ** -16 if variant == "bf16x3" else 2e-6)
