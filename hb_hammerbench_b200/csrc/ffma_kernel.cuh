@@ -19,6 +19,9 @@ struct FfmaShape {
   static constexpr int kAStage = BM * AS;
   static constexpr int kBStage = BK * BN;
   static constexpr int kSmemBytes = STAGES * (kAStage + kBStage) * 4;
+  // resident CTAs per SM the register budget is sized for: small register
+  // blocks (<= 64 accumulators) leave room for two 256-thread CTAs
+  static constexpr int kMinBlocks = (kThreads <= 128 || TM * TN <= 64) ? 2 : 1;
   static_assert(WM % 8 == 0 && WN % 16 == 0, "warp tile");
   static_assert(BK % 4 == 0, "BK");
   static_assert(((AS / 4) & 1) == 1, "A pad keeps 8 rows in distinct bank groups");

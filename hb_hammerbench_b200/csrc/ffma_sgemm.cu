@@ -27,7 +27,8 @@ namespace hbsg {
 
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR,
           bool TA = false, bool TB = false>
-__global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
+__global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads,
+                                  FfmaShape<BM, BN, BK, WM, WN, STAGES>::kMinBlocks)
     ffma_sgemm_kernel(FfmaParams p) {
   extern __shared__ __align__(16) float smem[];
   // Rasterised tile order: groups of `raster` tile rows, column-major inside
@@ -84,7 +85,7 @@ __global__ void splitk_reduce_kernel(const float* __restrict__ partial, float* _
 
 struct FfmaEntry {
   int bm, bn, bk, wm, wn, stages;
-  int threads, smem;
+  int threads, smem, per_sm;
   cudaError_t (*launch)(const FfmaParams&, dim3, cudaStream_t, bool vec);
 };
 
@@ -122,6 +123,7 @@ static cudaError_t launch_ffma_trans(const FfmaParams& p, dim3 grid, cudaStream_
   FfmaEntry {                                                                           \
     BM, BN, BK, WM, WN, ST, FfmaShape<BM, BN, BK, WM, WN, ST>::kThreads,                \
         FfmaShape<BM, BN, BK, WM, WN, ST>::kSmemBytes,                                  \
+        FfmaShape<BM, BN, BK, WM, WN, ST>::kMinBlocks,                                  \
         &launch_ffma<BM, BN, BK, WM, WN, ST, PAIR>                                      \
   }
 
@@ -134,7 +136,7 @@ static const FfmaEntry kFfmaTiles[] = {
     HBSG_FFMA_ENTRY(256, 128, 16, 64, 64, 4, true),   // 6: 8 warps, tall
     HBSG_FFMA_ENTRY(128, 128, 32, 64, 64, 3, true),   // 7: 4 warps, deeper K tile
     HBSG_FFMA_ENTRY(128, 128, 16, 64, 64, 4, false),  // 8: as 1 with scalar FMA
-    HBSG_FFMA_ENTRY(128, 256, 16, 64, 64, 4, false),  // 9: as 2 with scalar FMA
+    HBSG_FFMA_ENTRY(128, 128, 16, 64, 32, 4, true),   // 9: 8 warps, 8x8 per thread
 };
 static constexpr int kNumFfmaTiles = sizeof(kFfmaTiles) / sizeof(kFfmaTiles[0]);
 
@@ -163,7 +165,7 @@ int ffma_pick_tile(int M, int N, int K, int batch, int num_sms) {
   for (int idx : cand) {
     const FfmaEntry& e = kFfmaTiles[idx];
     const long tiles = (long)((M + e.bm - 1) / e.bm) * ((N + e.bn - 1) / e.bn) * batch;
-    const int per_sm = e.threads <= 128 ? 2 : 1;
+    const int per_sm = e.per_sm;
     const double slots = (double)num_sms * per_sm;
     const double waves = tiles / slots;
     const double eff = waves / ceil(waves);  // tail efficiency
@@ -240,7 +242,7 @@ int ffma_pick_splits(int tile_idx, int M, int N, int K, int batch, int requested
   if (requested > 0) return requested;
   const FfmaEntry& e = kFfmaTiles[tile_idx];
   const long tiles = (long)((M + e.bm - 1) / e.bm) * ((N + e.bn - 1) / e.bn) * batch;
-  const long slots = (long)sms * (e.threads <= 128 ? 2 : 1);
+  const long slots = (long)sms * e.per_sm;
   if (tiles * 2 > slots) return 1;
   const long by_k = K / (16 * e.bk) > 1 ? K / (16 * e.bk) : 1;
   const long s = (slots + tiles - 1) / tiles;

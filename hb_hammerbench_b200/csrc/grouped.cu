@@ -328,7 +328,8 @@ __global__ void __launch_bounds__(384, 1)
 }
 
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
-__global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads, 1)
+__global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads,
+                                  FfmaShape<BM, BN, BK, WM, WN, STAGES>::kMinBlocks)
     ffma_grouped_kernel(const GProblem* __restrict__ probs, const int4* __restrict__ tiles, int n) {
   extern __shared__ __align__(16) float smem[];
   for (int t = blockIdx.x; t < n; t += gridDim.x) {
@@ -387,6 +388,7 @@ __global__ void __launch_bounds__(256) gsplit_a_kernel(const GProblem* __restric
 
 // B: job {problem, k0, n0, 0}: one 64 x 64 block transposed through shared
 // memory into [N][Kp] (8 threads write each 128-byte output row segment).
+// (Jobs of four such blocks were measured 3x slower: fewer blocks in flight.)
 template <int P, bool SCALED>
 __global__ void __launch_bounds__(256) gsplit_b_kernel(const GProblem* __restrict__ probs,
                                                        const int4* __restrict__ jobs) {
@@ -595,14 +597,14 @@ static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* 
 
 // FFMA grouped instantiations mirror the FFMA tile table (ffma_sgemm.cu).
 struct GFfmaEntry {
-  int smem, threads;
+  int smem, threads, per_sm;
   const void* kv;
   const void* ks;
 };
 template <int BM, int BN, int BK, int WM, int WN, int ST, bool PAIR>
 static GFfmaEntry gffma_entry() {
   using S = FfmaShape<BM, BN, BK, WM, WN, ST>;
-  return {S::kSmemBytes, S::kThreads,
+  return {S::kSmemBytes, S::kThreads, S::kMinBlocks,
           reinterpret_cast<const void*>(&ffma_grouped_kernel<BM, BN, BK, WM, WN, ST, true, PAIR>),
           reinterpret_cast<const void*>(&ffma_grouped_kernel<BM, BN, BK, WM, WN, ST, false, PAIR>)};
 }
@@ -616,7 +618,7 @@ static GFfmaEntry gffma_table(int idx) {
     case 5: return gffma_entry<256, 128, 16, 64, 64, 4, true>();
     case 6: return gffma_entry<128, 128, 32, 64, 64, 3, true>();
     case 7: return gffma_entry<128, 128, 16, 64, 64, 4, false>();
-    default: return gffma_entry<128, 256, 16, 64, 64, 4, false>();
+    default: return gffma_entry<128, 128, 16, 64, 32, 4, true>();
   }
 }
 
@@ -900,7 +902,7 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   }
   if (e != cudaSuccess) return status_of(e);
 
-  const long slots = split ? sms : (long)sms * (gffma_table(pl->ffma_tile).threads <= 128 ? 2 : 1);
+  const long slots = split ? sms : (long)sms * gffma_table(pl->ffma_tile).per_sm;
   pl->grid = (int)std::max<long>(1, std::min<long>(slots, L.num_tiles));
   return HBSG_OK;
 }
