@@ -862,6 +862,7 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
     }
     pl->run.chunk_ktiles = tc_chunk_ktiles(P, cfg ? cfg->chunk_k : 0);
     pl->run.l2_ahead = tc_l2_ahead();
+    pl->run.l2_keep = tc_l2_keep();
     pl->run.wait_limit_ns = kWaitLimitNs;
     pl->run.debug_skip_loads = 0;
   }

@@ -55,6 +55,7 @@ int tc_read_and_clear_device_error();
 int grouped_read_and_clear_device_error();
 int tc_chunk_ktiles(int parts, int chunk_k);
 int tc_l2_ahead();
+int tc_l2_keep();
 bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, int box_rows);
 int tc_tile_bn(int idx);
 int tc_tile_pair(int idx);

@@ -324,6 +324,7 @@ cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int
   TcRun run;
   run.chunk_ktiles = tc_chunk_ktiles(e.parts, chunk_k);
   run.l2_ahead = tc_l2_ahead();
+  run.l2_keep = tc_l2_keep();
   run.debug_skip_loads = debug_skip_loads;
   run.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;
   const long items = (long)p.num_tiles * p.splits;
@@ -363,6 +364,16 @@ int tc_l2_ahead() {
     const char* e = getenv("HBSG_TC_L2_AHEAD");
     v = e ? atoi(e) : 0;  // off: measured slower at 2, 4 and 8 (extra TMA operations)
     if (v < 0) v = 0;
+  }
+  return v;
+}
+
+// Operand loads with an L2 evict-last policy (HBSG_TC_L2_KEEP=0/1, for tuning).
+int tc_l2_keep() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("HBSG_TC_L2_KEEP");
+    v = e ? (atoi(e) != 0) : 0;
   }
   return v;
 }

@@ -65,6 +65,23 @@ HBSG_DEV void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, 
       : "memory");
 }
 
+// Same load with an L2 cache policy (from createpolicy).
+HBSG_DEV void tma_load_3d_hint(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
+                               uint64_t* bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3, %4}], [%5], %6;\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar)),
+      "l"(policy)
+      : "memory");
+}
+
+HBSG_DEV uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 // L2 prefetch of one 3-D tensor box (no shared-memory destination, no
 // completion): keeps operand tiles warm in L2 ahead of the smem ring.
 HBSG_DEV void tma_prefetch_3d(const CUtensorMap* map, int c0, int c1, int c2) {
@@ -199,6 +216,7 @@ struct TileWork {
 // Settings shared by every tile of a launch.
 struct TcRun {
   int chunk_ktiles;                  // k-tiles accumulated in TMEM before draining
+  int l2_keep;                       // 1: operand loads carry an L2 evict-last policy
   int l2_ahead;                      // k-tiles prefetched into L2 ahead of the loads (0 = off)
   unsigned long long wait_limit_ns;  // bound of every mbarrier wait
   int debug_skip_loads;              // test hook: producer never loads (forces the timeout path)
@@ -261,6 +279,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
       bool ok = true;
       const CUtensorMap* last_ma = nullptr;
       int ready_prob = -1;
+      const uint64_t keep = l2_policy_evict_last();
       TileWork w;
       if (blockIdx.x < num_tiles) w = tiles.get(blockIdx.x);
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
@@ -294,8 +313,13 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           const uint32_t sa = base + s * S::kStageBytes;
           const uint32_t sb = sa + P * S::kABytes;
           mbar_arrive_expect_tx(&full[s], S::kStageBytes);
-          tma_load_3d(sa, w.ma, (w.kt0 + kt) * kBK, w.m0, 0, &full[s]);
-          tma_load_3d(sb, w.mb, (w.kt0 + kt) * kBK, w.n0, 0, &full[s]);
+          if (run.l2_keep) {
+            tma_load_3d_hint(sa, w.ma, (w.kt0 + kt) * kBK, w.m0, 0, &full[s], keep);
+            tma_load_3d_hint(sb, w.mb, (w.kt0 + kt) * kBK, w.n0, 0, &full[s], keep);
+          } else {
+            tma_load_3d(sa, w.ma, (w.kt0 + kt) * kBK, w.m0, 0, &full[s]);
+            tma_load_3d(sb, w.mb, (w.kt0 + kt) * kBK, w.n0, 0, &full[s]);
+          }
           if (run.l2_ahead > 0) {  // the k-tile l2_ahead steps further, possibly of the next tile
             const int ka = kt + (kt == 0 ? 1 : run.l2_ahead);
             const int kend = kt == 0 ? min(w.KT, 1 + run.l2_ahead) : ka + 1;
