@@ -249,7 +249,6 @@ __device__ __forceinline__ void tc_pair_body(const Tiles& tiles, const TcRun& ru
         if (lane == 0) mbar_arrive_remote(tempty_leader0 + 8u * buf);
       }
       if (!ok) break;
-      const int row = w.m0 + kBM * (int)rank + 32 * q + lane;
       const int col0 = w.n0 + h * COLS;
       int* wexp = col_exp + (warp - 2) * COLS;
       if constexpr (SCALED) {
@@ -259,30 +258,8 @@ __device__ __forceinline__ void tc_pair_body(const Tiles& tiles, const TcRun& ru
           wexp[i] = pow2_exp_of_bits(w.colmax[min(col0 + i, w.N - 1)]);
         __syncwarp();
       }
-      if (row < w.M) {
-        float* crow = w.C + (long)row * w.ldc;
-        int er = 0;
-        if constexpr (SCALED) er = pow2_exp_of_bits(w.rowmax[row]);
-        const bool vec = ((w.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(w.C) & 15) == 0);
-#pragma unroll
-        for (int j = 0; j < COLS; j += 4) {
-          float o[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            float x = sum[j + e];
-            if constexpr (SCALED) x = scale_pow2(x, er + wexp[j + e]);
-            o[e] = x;
-          }
-          const int c = col0 + j;
-          if (vec && c + 3 < w.N) {
-            *reinterpret_cast<float4*>(crow + c) = make_float4(o[0], o[1], o[2], o[3]);
-          } else {
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-              if (c + e < w.N) crow[c + e] = o[e];
-          }
-        }
-      }
+      store_rows_transposed<COLS, SCALED>(sum, w, w.m0 + kBM * (int)rank + 32 * q, col0, lane,
+                                          wexp);
     }
   }
 
