@@ -31,25 +31,37 @@ HBSG_DEV void split_value(float x, int e, __nv_bfloat16* out) {
 }
 
 // One 64 (k) x 64 (n) block of B (K x N, row stride ldb) split into
-// Bp[p][n][k0 .. k0+63] through the shared tile `tile` (256 threads).
-template <int P, bool SCALED>
-HBSG_DEV void split_b_block(const float* __restrict__ B, long ldb, int K, int N, int Kp,
-                            __nv_bfloat16* __restrict__ Bp, const uint32_t* __restrict__ colmax,
-                            int k0, int n0, float (*tile)[65]) {
+// Bp[p][n][k0 .. k0+63], in three steps that callers may interleave with
+// other blocks: split_b_load (16 values per thread into registers, coalesced
+// along n), split_b_to_tile (into the shared tile), split_b_from_tile (split
+// and store, 8 threads per 128-byte output row segment). 256 threads.
+HBSG_DEV void split_b_load(const float* __restrict__ B, long ldb, int K, int N, int k0, int n0,
+                           float* v) {
   const int tid = threadIdx.x;
-  // load: 64 rows (k) x 64 columns (n), coalesced along n
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     const int idx = tid + i * 256;
-    const int r = idx >> 6;
-    const int c = idx & 63;
-    const int k = k0 + r;
-    const int n = n0 + c;
-    tile[r][c] = (k < K && n < N) ? B[(long)k * ldb + n] : 0.0f;
+    const int k = k0 + (idx >> 6);
+    const int n = n0 + (idx & 63);
+    v[i] = (k < K && n < N) ? B[(long)k * ldb + n] : 0.0f;
   }
-  __syncthreads();
+}
+
+HBSG_DEV void split_b_to_tile(const float* v, float (*tile)[65]) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int idx = tid + i * 256;
+    tile[idx >> 6][idx & 63] = v[i];
+  }
+}
+
+template <int P, bool SCALED>
+HBSG_DEV void split_b_from_tile(int N, int Kp, __nv_bfloat16* __restrict__ Bp,
+                                const uint32_t* __restrict__ colmax, int k0, int n0,
+                                const float (*tile)[65]) {
+  const int tid = threadIdx.x;
   const long plane = (long)N * Kp;
-  // store: 8 threads per output row n, each 8 consecutive k
 #pragma unroll
   for (int pass = 0; pass < 2; ++pass) {
     const int j = pass * 32 + (tid >> 3);  // n offset
@@ -70,6 +82,17 @@ HBSG_DEV void split_b_block(const float* __restrict__ B, long ldb, int K, int N,
     for (int p = 0; p < P; ++p)
       *reinterpret_cast<uint4*>(dst + p * plane) = *reinterpret_cast<const uint4*>(parts[p]);
   }
+}
+
+template <int P, bool SCALED>
+HBSG_DEV void split_b_block(const float* __restrict__ B, long ldb, int K, int N, int Kp,
+                            __nv_bfloat16* __restrict__ Bp, const uint32_t* __restrict__ colmax,
+                            int k0, int n0, float (*tile)[65]) {
+  float v[16];
+  split_b_load(B, ldb, K, N, k0, n0, v);
+  split_b_to_tile(v, tile);
+  __syncthreads();
+  split_b_from_tile<P, SCALED>(N, Kp, Bp, colmax, k0, n0, tile);
 }
 
 }  // namespace hbsg
