@@ -860,8 +860,8 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
       for (int i = 0; i < count; ++i) {  // B split jobs: 64 x 64 blocks
         const GProblem& g = probs[i];
         if (g.M <= 0 || g.N <= 0 || sets.inl[i]) continue;
-        for (int k0 = 0; k0 < g.Kp; k0 += 64)
-          for (int n0 = 0; n0 < g.N; n0 += 64) jobs.push_back(make_int4(i, k0, n0, 0));
+        for (int n0 = 0; n0 < g.N; n0 += 64)  // n-major: neighbouring CTAs write one row run
+          for (int k0 = 0; k0 < g.Kp; k0 += 64) jobs.push_back(make_int4(i, k0, n0, 0));
       }
     }
     if (scaled) {
