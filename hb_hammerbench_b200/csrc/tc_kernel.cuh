@@ -191,10 +191,15 @@ HBSG_DEV int pow2_exp_of_bits(uint32_t bits) {
 }
 
 // x * 2^s, exact when 2^s is a normal float (one rounding otherwise, as ldexpf).
+// Out of line: the rare out-of-range case stays one call instruction at each
+// of the epilogue's many unrolled call sites, which keeps the kernel's code
+// (and so the MMA issuer's instruction-cache footprint) small.
+static __device__ __noinline__ float scale_pow2_slow(float x, int s) { return ldexpf(x, s); }
+
 HBSG_DEV float scale_pow2(float x, int s) {
   if (s == 0) return x;
   if (s >= -126 && s <= 127) return x * __uint_as_float((uint32_t)(s + 127) << 23);
-  return ldexpf(x, s);
+  return scale_pow2_slow(x, s);
 }
 
 // One output tile of work for the kernel body.
