@@ -95,7 +95,7 @@ static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg
     *tc = tile - ffma_num_tiles();
     if (*tc < 0 || *tc >= tc_num_tiles() || tc_tile_parts(*tc) != P) return false;
   } else {
-    *tc = tc_pick_tile(M, N, P, sms);
+    *tc = tc_pick_tile(M, N, K, P, sms, cfg ? cfg->split_k : 0);
   }
   *splits = tc_pick_splits(*tc, M, N, K, cfg ? cfg->split_k : 0, sms, kts);
   return true;

@@ -40,7 +40,7 @@ cudaError_t split_operand_b(const float* B, long ldb, int K, int N, int Kp, int 
 int tc_num_tiles();
 bool tc_tile_info(int idx, hbsg_tile_info* out);
 int tc_tile_parts(int idx);
-int tc_pick_tile(int M, int N, int parts, int sms);
+int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits);
 cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,
                       float* C, long ldc, const uint32_t* rowmax, const uint32_t* colmax,
                       int raster, int chunk_k, int sms, int debug_skip_loads,

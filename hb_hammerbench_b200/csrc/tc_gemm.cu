@@ -250,19 +250,57 @@ bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, in
   return tc_make_parts_map_impl(static_cast<CUtensorMap*>(map), parts, P, rows, Kp, box_rows);
 }
 
-int tc_pick_tile(int M, int N, int parts, int sms) {
+// K slices of the automatic schedule for `tiles` output tiles: enough
+// (tile, slice) work items to fill the concurrent slots when the output alone
+// has fewer than half as many tiles as slots, each slice keeping >= 8
+// k-tiles; `requested` > 0 overrides. Normalised so that no slice is empty.
+static int slices_for(long tiles, int KT, int slots, int requested, int* kt_per_split) {
+  int s = requested;
+  if (s <= 0) {
+    s = 1;
+    if (tiles * 2 <= slots) s = (int)std::min<long>((slots + tiles - 1) / tiles, std::max(1, KT / 8));
+  }
+  s = std::max(1, std::min(s, KT));
+  const int per = (KT + s - 1) / s;
+  if (kt_per_split) *kt_per_split = per;
+  return (KT + per - 1) / per;
+}
+
+static int ktiles_of(int K) {
+  const int KT = ((K + 31) / 32 * 32) / kBK;
+  return KT > 0 ? KT : 1;
+}
+
+// Tile shape for an M x N x K product: scored on the work items it yields
+// after K slicing (so a tall-K problem with a small output takes the wide,
+// efficient tile and fills the GPU with slices rather than narrow tiles),
+// the fraction of the last wave in use, the tile's operand bytes per MMA
+// flop, and the rows and columns wasted at the edges. Slices shorter than
+// kMinSliceKtiles are not counted: their FP32 partials, the reduction and
+// the pipeline refill outweigh the wider tile (measured at 1024^3, 1000^3
+// and 128x128x65536: 15-30 % slower than unsliced narrow tiles).
+static constexpr int kMinSliceKtiles = 16;
+
+int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits) {
+  const int KT = ktiles_of(K);
   int best = -1;
   double best_score = -1.0;
   for (int i = 0; i < kNumTcTiles; ++i) {
     const TcEntry& e = kTcTiles[i];
     if (e.parts != parts) continue;
     const int tbm = e.pair ? 2 * kBM : kBM;
+    const int slots = e.pair ? sms / 2 : sms;
     const long tiles = (long)((M + tbm - 1) / tbm) * ((N + e.bn - 1) / e.bn);
-    const double waves = (double)tiles / (e.pair ? sms / 2 : sms);
+    int per = KT;
+    int s = slices_for(tiles, KT, slots, requested_splits, &per);
+    if (requested_splits <= 0 && s > 1 && per < kMinSliceKtiles) s = 1;
+    const long items = tiles * s;
+    const double waves = (double)items / slots;
     const double eff = waves / ceil(waves);
     // shared-memory operand bytes per MMA flop (the single-CTA bound)
     const double width = e.pair ? 0.9 : e.bn == 256 ? 0.95 : e.bn == 128 ? 0.8 : 0.55;
-    const double waste = (double)N / (((N + e.bn - 1) / e.bn) * e.bn);
+    const double waste = (double)N / (((N + e.bn - 1) / e.bn) * e.bn) *
+                         ((double)M / (((M + tbm - 1) / tbm) * tbm));
     const double score = eff * width * waste * fmin(1.0, waves);
     if (score > best_score + 1e-9) {
       best_score = score;
@@ -272,26 +310,11 @@ int tc_pick_tile(int M, int N, int parts, int sms) {
   return best;
 }
 
-// Number of K slices for a problem: the requested count, or (0) enough slices
-// to give every SM a work item when the output has too few tiles, keeping at
-// least 8 k-tiles (256 of K) per slice. Returns the count actually used (no
-// empty slices) and the k-tiles per slice.
 int tc_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
   const TcEntry& e = kTcTiles[idx];
-  const int KT = ((K + 31) / 32 * 32) / kBK > 0 ? ((K + 31) / 32 * 32) / kBK : 1;
   const int tbm = e.pair ? 2 * kBM : kBM;
   const long tiles = (long)((M + tbm - 1) / tbm) * ((N + e.bn - 1) / e.bn);
-  const int slots = e.pair ? sms / 2 : sms;  // concurrent work items
-  int s = requested;
-  if (s <= 0) {
-    s = 1;
-    if (tiles * 2 <= slots) s = (int)std::min<long>((slots + tiles - 1) / tiles, std::max(1, KT / 8));
-  }
-  s = std::max(1, std::min(s, KT));
-  int per = (KT + s - 1) / s;
-  s = (KT + per - 1) / per;
-  *kt_per_split = per;
-  return s;
+  return slices_for(tiles, ktiles_of(K), e.pair ? sms / 2 : sms, requested, kt_per_split);
 }
 
 cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,
