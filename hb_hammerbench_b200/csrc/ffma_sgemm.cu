@@ -173,7 +173,11 @@ int ffma_pick_tile(int M, int N, int K, int batch, int num_sms) {
     // measured at 8192^3: 128x128 (2 CTAs/SM) is the fastest shape
     const double tile_eff = (e.bm * e.bn == 128 * 128) ? 1.0 : (e.bm * e.bn >= 128 * 256 ? 0.96 : 0.85);
     const double fill = fmin(1.0, tiles / slots);
-    const double score = eff * tile_eff * (fill < 1.0 ? fill : 1.0);
+    // share of the tile's rows and columns inside the matrix (a 128-wide tile
+    // on N = 64 computes twice the columns it stores)
+    const double inside = (double)M / (((M + e.bm - 1) / e.bm) * e.bm) *
+                          ((double)N / (((N + e.bn - 1) / e.bn) * e.bn));
+    const double score = eff * tile_eff * (fill < 1.0 ? fill : 1.0) * inside;
     if (score > best + 1e-9) {
       best = score;
       best_idx = idx;
