@@ -236,7 +236,9 @@ def test_device_wait_timeout_is_reported_and_recoverable(hb):
 
 
 @pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
-@pytest.mark.parametrize("m,n,k,splits", [(256, 256, 65536, 0), (128, 256, 20000, 7), (300, 100, 4096, 3)])
+@pytest.mark.parametrize("m,n,k,splits", [(256, 256, 65536, 0), (256, 1024, 32768, 0),
+                                           (2048, 512, 8192, 0), (128, 256, 20000, 7),
+                                           (300, 100, 4096, 3)])
 def test_split_k(hb, variant, m, n, k, splits):
     import torch
     A = _rand((m, k), k + 1)
