@@ -21,7 +21,8 @@
 //   warps 2-9   epilogue: thread (quadrant q, half h) owns TMEM lane 32q+lane
 //               (= output row) and BN/2 columns; it adds each drained chunk
 //               to its register sums, releases the buffer, and at the end of
-//               the tile scales by 2^(row exp + col exp) and stores C.
+//               the tile scales by 2^(row exp + col exp) and stores C through
+//               an 8-lane float4 transpose (128-byte row segments per store).
 // No TMA multicast is used; every CTA fetches its own tiles.
 // Every wait is bounded: after kWaitLimitNs the kernel records
 // HBSG_ERR_DEVICE_TIMEOUT in the device error flag and unwinds.
