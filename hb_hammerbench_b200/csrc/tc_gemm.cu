@@ -125,18 +125,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(320, 1)
 // ---------------------------------------------------------------------------
 // Host side: tensor maps, tile table, launch.
 
+// Resolved once; function-local static initialisation is thread-safe, so
+// concurrent first calls from several host threads all see the pointer.
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
+      return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+  }();
   return fn;
 }
 
@@ -383,22 +383,20 @@ int tc_chunk_ktiles(int parts, int chunk_k) {
 // k-tiles the producer prefetches into L2 ahead of its loads
 // (HBSG_TC_L2_AHEAD overrides the default, for tuning).
 int tc_l2_ahead() {
-  static int v = -1;
-  if (v < 0) {
+  static const int v = [] {
     const char* e = getenv("HBSG_TC_L2_AHEAD");
-    v = e ? atoi(e) : 0;  // off: measured slower at 2, 4 and 8 (extra TMA operations)
-    if (v < 0) v = 0;
-  }
+    const int x = e ? atoi(e) : 0;  // off: measured slower at 2, 4 and 8 (extra TMA operations)
+    return x < 0 ? 0 : x;
+  }();
   return v;
 }
 
 // Operand loads with an L2 evict-last policy (HBSG_TC_L2_KEEP=0/1, for tuning).
 int tc_l2_keep() {
-  static int v = -1;
-  if (v < 0) {
+  static const int v = [] {
     const char* e = getenv("HBSG_TC_L2_KEEP");
-    v = e ? (atoi(e) != 0) : 0;
-  }
+    return e ? (atoi(e) != 0 ? 1 : 0) : 0;
+  }();
   return v;
 }
 
