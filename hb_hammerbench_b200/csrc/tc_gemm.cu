@@ -299,7 +299,7 @@ int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits) 
     const double waves = (double)items / slots;
     const double eff = waves / ceil(waves);
     // shared-memory operand bytes per MMA flop (the single-CTA bound)
-    const double width = e.pair ? 0.9 : e.bn == 256 ? 0.95 : e.bn == 128 ? 0.8 : 0.55;
+    const double width = e.pair ? 0.9 : e.bn == 256 ? 0.95 : e.bn == 192 ? 0.9 : e.bn == 128 ? 0.8 : 0.55;
     const double waste = (double)N / (((N + e.bn - 1) / e.bn) * e.bn) *
                          ((double)M / (((M + tbm - 1) / tbm) * tbm));
     const double score = eff * width * waste * fmin(1.0, waves);

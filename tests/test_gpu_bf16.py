@@ -263,7 +263,7 @@ def test_split_k_workspace_reported(hb):
     assert need_auto > need_one  # the heuristic splits this shape (2 tiles)
 
 
-@pytest.mark.parametrize("variant,pair_tile,single_tile", [("bf16x6", 16, 10), ("bf16x3", 17, 13)])
+@pytest.mark.parametrize("variant,pair_tile,single_tile", [("bf16x6", 18, 10), ("bf16x3", 19, 13)])
 @pytest.mark.parametrize("m,n,k", [(256, 256, 64), (1000, 700, 300), (2048, 1536, 1024)])
 def test_cta_pair_tiles_match_single_cta(hb, variant, pair_tile, single_tile, m, n, k):
     # the CTA-pair kernel (tcgen05 cta_group::2, 256-row tiles) issues the same
