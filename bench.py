@@ -138,29 +138,43 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference host_mm loop on a row sample
 
-def cpu_baseline(n: int, seconds: float = 12.0, threads: int = 0) -> dict:
-    import numpy as np
+class _CpuSampler:
+    """The reference's host_mm loop (the oracle port) on a bounded row sample
+    of the n^3 product: B and the per-row cost are prepared once, and each
+    sample() times `seconds` worth of rows (the cost is linear in rows)."""
 
-    from oracle import oracle
-    rng = np.random.Generator(np.random.PCG64(42))
-    B = rng.uniform(-1, 1, size=(n, n)).astype(np.float32)
-    nthreads = threads or len(os.sched_getaffinity(0))
-    rows = nthreads
-    A = rng.uniform(-1, 1, size=(rows, n)).astype(np.float32)
-    t0 = time.perf_counter()
-    oracle.host_mm(A, B, threads=nthreads)
-    per_row = (time.perf_counter() - t0) / rows
-    rows = int(max(nthreads, min(n, seconds / max(per_row, 1e-9))))
-    rows = max(nthreads, rows // nthreads * nthreads)
-    A = rng.uniform(-1, 1, size=(rows, n)).astype(np.float32)
-    t0 = time.perf_counter()
-    oracle.host_mm(A, B, threads=nthreads)
-    dt = time.perf_counter() - t0
-    flops = 2.0 * rows * n * n
-    return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": nthreads, "kind": "port",
-            "sample": f"host_mm loop (apps/sgemm/main.cpp:15-26 restated, gcc -O3) on {rows} of "
-                      f"{n} output rows of the {n}^3 product, {dt:.1f} s, OpenMP over rows; "
-                      "cost is linear in rows"}
+    def __init__(self, n: int, threads: int = 0):
+        import numpy as np
+
+        from oracle import oracle
+        self.oracle = oracle
+        self.n = n
+        self.rng = np.random.Generator(np.random.PCG64(42))
+        self.B = self.rng.uniform(-1, 1, size=(n, n)).astype(np.float32)
+        self.nthreads = threads or len(os.sched_getaffinity(0))
+        A = self.rng.uniform(-1, 1, size=(self.nthreads, n)).astype(np.float32)
+        t0 = time.perf_counter()
+        oracle.host_mm(A, self.B, threads=self.nthreads)
+        self.per_row = (time.perf_counter() - t0) / self.nthreads
+
+    def sample(self, seconds: float) -> dict:
+        import numpy as np
+        n, nt = self.n, self.nthreads
+        rows = int(max(nt, min(n, seconds / max(self.per_row, 1e-9))))
+        rows = max(nt, rows // nt * nt)
+        A = self.rng.uniform(-1, 1, size=(rows, n)).astype(np.float32)
+        t0 = time.perf_counter()
+        self.oracle.host_mm(A, self.B, threads=nt)
+        dt = time.perf_counter() - t0
+        flops = 2.0 * rows * n * n
+        return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": nt, "kind": "port",
+                "sample": f"host_mm loop (apps/sgemm/main.cpp:15-26 restated, gcc -O3) on {rows} of "
+                          f"{n} output rows of the {n}^3 product, {dt:.1f} s, OpenMP over rows; "
+                          "cost is linear in rows"}
+
+
+def cpu_baseline(n: int, seconds: float = 12.0, threads: int = 0) -> dict:
+    return _CpuSampler(n, threads).sample(seconds)
 
 
 # ---------------------------------------------------------------------------
@@ -196,8 +210,9 @@ def run_reference(args) -> None:
     per_step = max(2.0, 60.0 / (args.steps + args.warmup))
     vals = []
     cb = None
+    sampler = _CpuSampler(n)
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(n, seconds=per_step)
+        cb = sampler.sample(per_step)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = statistics.median(vals)
