@@ -27,7 +27,7 @@ def L():
 
 
 def test_library_loads(L):
-    assert L.lib().hbsg_version() == 100
+    assert L.lib().hbsg_version() == 101
 
 
 def test_exports_every_declared_symbol(L):

@@ -205,7 +205,7 @@ def test_strided_output(hb):
     assert torch.isnan(buf[:, :3]).all() and torch.isnan(buf[:, n + 3:]).all()
 
 
-@pytest.mark.parametrize("tile", [10, 11, 12, 13, 14, 15])
+@pytest.mark.parametrize("tile", [10, 11, 12, 13, 14, 15, 16, 17])
 def test_every_tensor_core_tile(hb, tile):
     info = [t for t in hb.tiles() if t["tile"] == tile][0]
     assert info["family"] == "bf16"
