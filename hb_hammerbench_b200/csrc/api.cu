@@ -10,12 +10,12 @@
 namespace hbsg {
 
 static std::mutex g_dev_mu;
-static int g_sms[64];
-static int g_ok[64];  // 0 unknown, 1 sm_100, -1 other
+static int g_sms[kMaxDevices];
+static int g_ok[kMaxDevices];  // 0 unknown, 1 sm_100, -1 other
 
 int current_device_sms(int* device_out) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
     return -1;
   }
@@ -33,13 +33,14 @@ int current_device_sms(int* device_out) {
   return g_ok[dev] == 1 ? g_sms[dev] : -1;
 }
 
-bool set_smem_once(const void* func, int bytes, uint32_t* device_mask) {
+bool set_smem_once(const void* func, int bytes, uint64_t* device_mask) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 32) return false;
-  if (__atomic_load_n(device_mask, __ATOMIC_ACQUIRE) & (1u << dev)) return true;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+  const uint64_t bit = 1ull << dev;
+  if (__atomic_load_n(device_mask, __ATOMIC_ACQUIRE) & bit) return true;
   if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
     return false;
-  __atomic_fetch_or(device_mask, 1u << dev, __ATOMIC_ACQ_REL);
+  __atomic_fetch_or(device_mask, bit, __ATOMIC_ACQ_REL);
   return true;
 }
 
@@ -81,37 +82,70 @@ static SplitLayout split_layout(int M, int N, int K, int variant) {
   return L;
 }
 
-// Global tile ids: 1..F are the FFMA family, F+1..F+T the tensor-core family.
-static int total_tiles() { return ffma_num_tiles() + tc_num_tiles(); }
+// Workspace layout of a fused-split schedule: only the scaled forms' row and
+// column maxima (the parts never reach HBM), then the K-slice partials.
+static SplitLayout fused_layout(int M, int N, int variant) {
+  SplitLayout L{};
+  L.rowmax_off = 0;
+  L.colmax_off = scaled_of(variant) ? align256((size_t)M * 4) : 0;
+  L.total = L.colmax_off + (scaled_of(variant) ? align256((size_t)N * 4) : 0);
+  L.a_off = L.b_off = L.total;
+  return L;
+}
+
+// Global tile ids: 1..F are the FFMA family, F+1..F+T the split-BF16
+// tensor-core family with a split pass, F+T+1..F+T+U the split-BF16 family
+// with the split fused into the product kernel.
+static int total_tiles() { return ffma_num_tiles() + tc_num_tiles() + fused_num_tiles(); }
+
+struct TcChoice {
+  bool fused;  // idx indexes the fused table (else the tensor-core table)
+  int idx;
+  int splits, kts;
+};
 
 // Tensor-core tile and K-slice count for a split-BF16 problem (shared by the
 // workspace query and the dispatcher so both agree). Returns false when an
-// explicitly requested tile does not fit the variant.
+// explicitly requested tile does not fit the variant or the operand layout
+// (the fused kernels take row-major operands only).
 static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg, int sms,
-                        int* tc, int* splits, int* kts) {
+                        bool transposed, TcChoice* ch) {
   const int P = parts_of(variant);
   const int tile = cfg && cfg->tile > 0 ? cfg->tile - 1 : -1;
+  const int req = cfg ? cfg->split_k : 0;
+  ch->fused = false;
   if (tile >= 0) {
-    *tc = tile - ffma_num_tiles();
-    if (*tc < 0 || *tc >= tc_num_tiles() || tc_tile_parts(*tc) != P) return false;
+    const int t = tile - ffma_num_tiles();
+    if (t >= tc_num_tiles()) {
+      ch->fused = true;
+      ch->idx = t - tc_num_tiles();
+      if (transposed || ch->idx >= fused_num_tiles() || fused_tile_parts(ch->idx) != P) return false;
+    } else {
+      ch->idx = t;
+      if (t < 0 || tc_tile_parts(t) != P) return false;
+    }
   } else {
-    *tc = tc_pick_tile(M, N, K, P, sms, cfg ? cfg->split_k : 0);
+    ch->idx = tc_pick_tile(M, N, K, P, sms, req);
   }
-  *splits = tc_pick_splits(*tc, M, N, K, cfg ? cfg->split_k : 0, sms, kts);
+  ch->splits = ch->fused ? fused_pick_splits(ch->idx, M, N, K, req, sms, &ch->kts)
+                         : tc_pick_splits(ch->idx, M, N, K, req, sms, &ch->kts);
   return true;
 }
 
-static size_t workspace_needed(int M, int N, int K, int batch, int variant, const hbsg_config* cfg) {
+static size_t workspace_needed(int M, int N, int K, int batch, int variant, const hbsg_config* cfg,
+                               bool transposed = false) {
   if (variant == HBSG_FFMA) {
     const int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
     return ffma_workspace_bytes(M, N, batch, splits);
   }
-  int sms = current_device_sms(nullptr);
-  if (sms < 0) sms = 148;
-  int tc = 0, splits = 1, kts = 0;
-  if (!tc_schedule(M, N, K, variant, cfg, sms, &tc, &splits, &kts)) return 0;
-  const size_t partial = splits > 1 ? align256((size_t)splits * M * N * 4) : 0;
-  return split_layout(M, N, K, variant).total + partial;
+  // The schedule (and so the split-K partial buffer) depends on the SM count
+  // of the device the product will run on: sizes are for the current device.
+  const int sms = current_device_sms(nullptr);
+  if (sms < 0) return 0;
+  TcChoice ch;
+  if (!tc_schedule(M, N, K, variant, cfg, sms, transposed, &ch)) return 0;
+  const size_t partial = ch.splits > 1 ? align256((size_t)ch.splits * M * N * 4) : 0;
+  return (ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant)).total + partial;
 }
 
 // Core dispatcher for one (possibly batched) GEMM.
@@ -161,17 +195,20 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
     p.K = K;
     p.splits = splits;
     p.raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 8;
-    return status_from(ffma_launch(tile, p, batch, st, trans_a ? 1 : 0, trans_b ? 1 : 0));
+    return status_from(ffma_launch(tile, p, batch, sms, st, trans_a ? 1 : 0, trans_b ? 1 : 0));
   }
 
   // ---- split-BF16 on the tensor cores ----
   const int P = parts_of(variant);
   const bool scaled = scaled_of(variant);
-  int tc = -1, splits = 1, kts = 0;
-  if (!tc_schedule(M, N, K, variant, cfg, sms, &tc, &splits, &kts)) return HBSG_ERR_UNSUPPORTED;
-  const SplitLayout L = split_layout(M, N, K, variant);
+  TcChoice ch;
+  if (!tc_schedule(M, N, K, variant, cfg, sms, trans_a || trans_b, &ch))
+    return HBSG_ERR_UNSUPPORTED;
+  const int tc = ch.idx, splits = ch.splits;
+  const SplitLayout L = ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant);
   const size_t partial_bytes = splits > 1 ? align256((size_t)splits * M * N * 4) : 0;
-  if (!ws || ws_bytes < L.total + partial_bytes || (reinterpret_cast<uintptr_t>(ws) & 255))
+  if (L.total + partial_bytes > 0 &&
+      (!ws || ws_bytes < L.total + partial_bytes || (reinterpret_cast<uintptr_t>(ws) & 255)))
     return HBSG_ERR_WORKSPACE;
   uint8_t* w = static_cast<uint8_t*>(ws);
   void* Ap = w + L.a_off;
@@ -181,6 +218,38 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   const int flags = cfg ? cfg->flags : 0;
   const int raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 0;
   const int chunk = cfg && cfg->chunk_k > 0 ? cfg->chunk_k : 0;
+  if (ch.fused) {
+    // The split runs inside the product kernel; the workspace holds only the
+    // scaled forms' maxima (PRESPLIT_A / _B: already current) and partials.
+    for (int b = 0; b < batch; ++b) {
+      const float* Ab = A + b * strideA;
+      const float* Bb = B + b * strideB;
+      cudaError_t e = cudaSuccess;
+      if (scaled && !(flags & HBSG_FLAG_PRESPLIT_A)) e = maxabs_rows(Ab, lda, M, K, rowmax, st);
+      if (e == cudaSuccess && scaled && !(flags & HBSG_FLAG_PRESPLIT_B))
+        e = maxabs_cols(Bb, ldb, K, N, colmax, st);
+      if (e != cudaSuccess) return status_from(e);
+      if (flags & HBSG_FLAG_SPLIT_ONLY) continue;
+      FusedParams fp{};
+      fp.A = Ab;
+      fp.B = Bb;
+      fp.C = C + b * strideC;
+      fp.lda = lda;
+      fp.ldb = ldb;
+      fp.ldc = ldc;
+      fp.M = M;
+      fp.N = N;
+      fp.K = K;
+      fp.splits = splits;
+      fp.kt_per_split = ch.kts;
+      fp.rowmax = rowmax;
+      fp.colmax = colmax;
+      e = fused_launch(tc, fp, raster, chunk, sms, 0, st,
+                       reinterpret_cast<float*>(w + L.total));
+      if (e != cudaSuccess) return status_from(e);
+    }
+    return HBSG_OK;
+  }
   for (int b = 0; b < batch; ++b) {
     const float* Ab = A + b * strideA;
     const float* Bb = B + b * strideB;
@@ -256,6 +325,12 @@ size_t hbsg_gemm_workspace_size(int m, int n, int k, int variant, const hbsg_con
   return workspace_needed(m, n, k, 1, variant, cfg);
 }
 
+size_t hbsg_gemm_workspace_size_ex(int trans_a, int trans_b, int m, int n, int k, int variant,
+                                   const hbsg_config* cfg) {
+  if (m <= 0 || n <= 0 || k < 0 || !variant_valid(variant)) return 0;
+  return workspace_needed(m, n, k, 1, variant, cfg, trans_a || trans_b);
+}
+
 int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* out) {
   if (!out || m <= 0 || n <= 0 || k < 0) return HBSG_ERR_INVALID_ARG;
   if (!variant_valid(variant) || variant == HBSG_FFMA) return HBSG_ERR_UNSUPPORTED;
@@ -276,8 +351,11 @@ int hbsg_tile_describe(int tile, hbsg_tile_info* out) {
   if (!out) return HBSG_ERR_INVALID_ARG;
   if (tile < 1 || tile > total_tiles()) return HBSG_ERR_INVALID_ARG;
   const int idx = tile - 1;
-  const bool ok = idx < ffma_num_tiles() ? ffma_tile_info(idx, out)
-                                         : tc_tile_info(idx - ffma_num_tiles(), out);
+  const int F = ffma_num_tiles(), T = tc_num_tiles();
+  const bool ok = idx < F       ? ffma_tile_info(idx, out)
+                  : idx < F + T ? tc_tile_info(idx - F, out)
+                                : fused_tile_info(idx - F - T, out);
+  out->fused = idx >= F + T ? 1 : 0;
   return ok ? HBSG_OK : HBSG_ERR_INVALID_ARG;
 }
 
@@ -301,7 +379,8 @@ int hbsg_check_device(hbsg_stream_t stream) {
   if (e != cudaSuccess) return status_from(e);
   const int f1 = tc_read_and_clear_device_error();
   const int f2 = grouped_read_and_clear_device_error();
-  return f1 != HBSG_OK ? f1 : f2;
+  const int f3 = fused_read_and_clear_device_error();
+  return f1 != HBSG_OK ? f1 : f2 != HBSG_OK ? f2 : f3;
 }
 
 int hbsg_debug_timeout_probe(void* workspace, size_t workspace_bytes, hbsg_stream_t stream) {
@@ -323,6 +402,6 @@ int hbsg_debug_timeout_probe(void* workspace, size_t workspace_bytes, hbsg_strea
   return status_from(e);
 }
 
-int hbsg_version(void) { return 100; }
+int hbsg_version(void) { return 101; }
 
 }  // extern "C"

@@ -95,7 +95,7 @@ static cudaError_t launch_ffma(const FfmaParams& p, dim3 grid, cudaStream_t st, 
   auto kv = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, true, PAIR>;
   auto ks = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, PAIR>;
   auto k = vec ? kv : ks;
-  static uint32_t mask_v = 0, mask_s = 0;
+  static uint64_t mask_v = 0, mask_s = 0;
   if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, vec ? &mask_v : &mask_s))
     return cudaErrorInvalidValue;
   k<<<grid, S::kThreads, S::kSmemBytes, st>>>(p);
@@ -111,7 +111,7 @@ static cudaError_t launch_ffma_trans(const FfmaParams& p, dim3 grid, cudaStream_
   auto k01 = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, true, false, true>;
   auto k11 = ffma_sgemm_kernel<BM, BN, BK, WM, WN, STAGES, false, true, true, true>;
   auto k = ta && tb ? k11 : ta ? k10 : k01;
-  static uint32_t masks[3] = {0, 0, 0};
+  static uint64_t masks[3] = {0, 0, 0};
   const int slot = ta && tb ? 2 : ta ? 0 : 1;
   if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, &masks[slot]))
     return cudaErrorInvalidValue;
@@ -190,7 +190,8 @@ size_t ffma_workspace_bytes(int M, int N, int batch, int splits) {
   return splits > 1 ? (size_t)M * N * batch * splits * sizeof(float) : 0;
 }
 
-cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st, int ta, int tb) {
+cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, int sms, cudaStream_t st, int ta,
+                        int tb) {
   // transposed operands: 128 x 128 or 64 x 64 tiles (the closest of the two)
   if (ta || tb) {
     const FfmaEntry& big = kFfmaTiles[0];
@@ -226,7 +227,7 @@ cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st, 
     err = e.launch(p, grid, st, vec);
   }
   if (err != cudaSuccess || p.splits == 1) return err;
-  return splitk_reduce(p.partial, p.C, p.M, p.N, p.ldc, p.strideC, p.splits, batch, 148, st);
+  return splitk_reduce(p.partial, p.C, p.M, p.N, p.ldc, p.strideC, p.splits, batch, sms, st);
 }
 
 cudaError_t splitk_reduce(const float* partial, float* C, int M, int N, long ldc, long strideC,

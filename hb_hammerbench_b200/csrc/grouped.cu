@@ -663,10 +663,10 @@ static const GTcEntry kGTc[] = {HBSG_TC_TILE_LIST(HBSG_GTC_ENTRY)};
            reinterpret_cast<const void*>(&tc_grouped_inline_kernel<P, BN, ST, false>),      \
            reinterpret_cast<const void*>(&tc_grouped_inline_kernel<P, BN, ST, true>)},
 static const GTcEntry kGTcInline[] = {HBSG_TC_TILE_LIST(HBSG_GTCI_ENTRY)};
-static uint32_t g_tci_masks[sizeof(kGTcInline) / sizeof(kGTcInline[0])][2];
+static uint64_t g_tci_masks[sizeof(kGTcInline) / sizeof(kGTcInline[0])][2];
 
-static uint32_t g_ffma_masks[9][2];
-static uint32_t g_tc_masks[sizeof(kGTc) / sizeof(kGTc[0])][2];
+static uint64_t g_ffma_masks[9][2];
+static uint64_t g_tc_masks[sizeof(kGTc) / sizeof(kGTc[0])][2];
 
 // Launches of one grouped product on `st` (no host synchronisation, no
 // allocation: capturable).

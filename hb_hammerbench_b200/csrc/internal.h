@@ -29,8 +29,8 @@ int ffma_num_tiles();
 bool ffma_tile_info(int idx, hbsg_tile_info* out);
 int ffma_pick_tile(int M, int N, int K, int batch, int num_sms);
 size_t ffma_workspace_bytes(int M, int N, int batch, int splits);
-cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, cudaStream_t st, int ta = 0,
-                        int tb = 0);
+cudaError_t ffma_launch(int tile_idx, FfmaParams p, int batch, int sms, cudaStream_t st,
+                        int ta = 0, int tb = 0);
 
 // ---- split-BF16 family ----------------------------------------------------------
 cudaError_t split_operand_a(const float* A, long lda, int M, int K, int Kp, int parts, bool scaled,
@@ -60,12 +60,46 @@ bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, in
 int tc_tile_bn(int idx);
 int tc_tile_pair(int idx);
 
+// ---- fused split-BF16 family (tc_fused.cu) ---------------------------------------
+struct FusedParams {
+  const float* A;  // M x K, row stride lda
+  const float* B;  // K x N, row stride ldb
+  float* C;        // M x N, row stride ldc (the launch redirects slices to partials)
+  long lda, ldb, ldc;
+  int M, N, K;
+  int tiles_m, tiles_n, num_tiles;
+  int raster;
+  int splits;        // K slices (1 = none)
+  int kt_per_split;  // k-tiles (of 32) per slice
+  const uint32_t* rowmax;  // scaled forms: FP32 bit patterns of max|A row| / max|B column|
+  const uint32_t* colmax;
+};
+int fused_num_tiles();
+bool fused_tile_info(int idx, hbsg_tile_info* out);
+int fused_tile_parts(int idx);
+int fused_tile_bn(int idx);
+int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split);
+// C = A*B on fused entry idx; partial: [splits][M][N] FP32 when p.splits > 1.
+cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sms,
+                         unsigned long long wait_limit_ns, cudaStream_t st, float* partial);
+int fused_read_and_clear_device_error();
+// K slices of the automatic schedule for `tiles` output tiles on `slots`
+// concurrent work slots (requested > 0 overrides); shared by both families.
+int tc_slices(long tiles, int K, int slots, int requested, int* kt_per_split);
+// Row / column maxima of |x| (FP32 bit patterns) for the scaled forms.
+cudaError_t maxabs_rows(const float* A, long lda, int M, int K, uint32_t* rowmax, cudaStream_t st);
+cudaError_t maxabs_cols(const float* B, long ldb, int K, int N, uint32_t* colmax, cudaStream_t st);
+
 // ---- device state -------------------------------------------------------------
+// Device ordinals the per-device tables cover (one bit each in a uint64_t).
+static constexpr int kMaxDevices = 64;
+
 // Returns the SM count of the current device (cached per device), or -1 when
-// no sm_100 device is current.
+// no sm_100 device is current (or its ordinal is >= kMaxDevices).
 int current_device_sms(int* device_out);
 
-// Sets a kernel's dynamic shared memory limit once per device.
-bool set_smem_once(const void* func, int bytes, uint32_t* device_mask);
+// Sets a kernel's dynamic shared memory limit once per device (one bit of
+// *device_mask per device ordinal).
+bool set_smem_once(const void* func, int bytes, uint64_t* device_mask);
 
 }  // namespace hbsg

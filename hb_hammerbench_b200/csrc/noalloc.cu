@@ -28,24 +28,36 @@ namespace hbsg {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HBSG_NOALLOC_SCRATCH_BYTES];
 
 static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[64];
+static void* g_noalloc_addr[kMaxDevices];
 
-// Device address of the scratch array on the current device (looked up once).
+static int lookup_scratch(void** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return HBSG_ERR_CUDA;
+  }
+  *out = p;
+  return HBSG_OK;
+}
+
+// Device address of the scratch array on the current device: looked up on the
+// first call made on each device and kept for the life of the process. The
+// cached address belongs to the device's primary context, so it does not
+// survive cudaDeviceReset (the module is loaded again, possibly elsewhere);
+// callers that reset a device must not use this entry point afterwards.
+// Device ordinals beyond the table are looked up on every call.
 static int noalloc_scratch(void** out) {
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     cudaGetLastError();
     return HBSG_ERR_NO_DEVICE;
   }
+  if (dev >= kMaxDevices) return lookup_scratch(out);
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return HBSG_ERR_CUDA;
-    }
-    g_noalloc_addr[dev] = p;
+    const int st = lookup_scratch(&g_noalloc_addr[dev]);
+    if (st != HBSG_OK) return st;
   }
   *out = g_noalloc_addr[dev];
   return HBSG_OK;

@@ -35,11 +35,12 @@ _ref = None
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compile liboracle.so, and the reference host_mm library when the
-    reference tree is present."""
+    """Compile liboracle.so, and the reference host_mm library when a
+    reference checkout is given (argument, else $HB_REFERENCE_ROOT) and holds
+    apps/sgemm/main.cpp."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    root = reference_root or "/root/reference"
-    if os.path.isfile(os.path.join(root, "apps", "sgemm", "main.cpp")):
+    root = reference_root or os.environ.get("HB_REFERENCE_ROOT")
+    if root and os.path.isfile(os.path.join(root, "apps", "sgemm", "main.cpp")):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={root}"], check=True)
 
 
