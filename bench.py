@@ -29,7 +29,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -40,7 +39,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "effective FP32 TFLOP/s at stated error vs FP64: split-BF16 TC vs plain FFMA, 1 B200"
-SMS = 148
+SMS = 148  # B200 SM count, for the derived FP32 figure reported beside the measured one
 FP32_LANES_PER_SM = 128
 PRODUCTS = {"bf16x3": 3, "bf16x6": 6, "bf16x3_scaled": 3, "bf16x6_scaled": 6}
 
@@ -56,13 +55,14 @@ def _peaks():
 
 
 def _profile_traffic(name: str):
-    """DRAM bytes per launch recorded from an ncu capture in profiles/<name>.md
-    (line `dram_bytes_per_launch: <int>`), or None."""
-    p = os.path.join(ROOT, "profiles", name + ".md")
-    if not os.path.exists(p):
+    """DRAM bytes per launch of a kernel and workload from one ncu capture, as
+    recorded in profiles/traffic.json (key: kernel and workload), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        entry = json.load(open(p)).get(name)
+    except (OSError, ValueError):
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9]+)", open(p).read())
-    return int(m.group(1)) if m else None
+    return int(entry["dram_bytes_per_launch"]) if entry else None
 
 
 # ---------------------------------------------------------------------------
@@ -152,16 +152,21 @@ class _CpuSampler:
         self.rng = np.random.Generator(np.random.PCG64(42))
         self.B = self.rng.uniform(-1, 1, size=(n, n)).astype(np.float32)
         self.nthreads = threads or len(os.sched_getaffinity(0))
-        A = self.rng.uniform(-1, 1, size=(self.nthreads, n)).astype(np.float32)
+        nt = self.nthreads
+        # one untimed pass starts the thread pool and touches B, then the
+        # per-row cost is timed over two rows per thread
+        oracle.host_mm(self.rng.uniform(-1, 1, size=(nt, n)).astype(np.float32), self.B,
+                       threads=nt)
+        A = self.rng.uniform(-1, 1, size=(2 * nt, n)).astype(np.float32)
         t0 = time.perf_counter()
-        oracle.host_mm(A, self.B, threads=self.nthreads)
-        self.per_row = (time.perf_counter() - t0) / self.nthreads
+        oracle.host_mm(A, self.B, threads=nt)
+        self.per_row = (time.perf_counter() - t0) / (2 * nt)
 
-    def sample(self, seconds: float) -> dict:
+    def sample(self, seconds: float, min_rows: int = 0) -> dict:
         import numpy as np
         n, nt = self.n, self.nthreads
-        rows = int(max(nt, min(n, seconds / max(self.per_row, 1e-9))))
-        rows = max(nt, rows // nt * nt)
+        rows = int(max(nt, min_rows, min(n, seconds / max(self.per_row, 1e-9))))
+        rows = min(n, max(nt, -(-rows // nt) * nt))
         A = self.rng.uniform(-1, 1, size=(rows, n)).astype(np.float32)
         t0 = time.perf_counter()
         self.oracle.host_mm(A, self.B, threads=nt)
@@ -202,6 +207,9 @@ def _dist():
     return ws, rank, local
 
 
+REF_MIN_ROWS = 128  # rows of the product timed per reference step, at least
+
+
 def run_reference(args) -> None:
     ws, rank, _ = _dist()
     if rank != 0:
@@ -212,7 +220,7 @@ def run_reference(args) -> None:
     cb = None
     sampler = _CpuSampler(n)
     for i in range(args.warmup + args.steps):
-        cb = sampler.sample(per_step)
+        cb = sampler.sample(per_step, min_rows=REF_MIN_ROWS)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = statistics.median(vals)
@@ -341,7 +349,8 @@ def run_ours(args) -> None:
         f_steps = max(3, args.steps // 2)
         f_val = ws * flops * f_steps / (f_total * 1e-3) / 1e12
         ffma = {"value": f_val, "unit": "TFLOP/s", "ms_per_step": f_total / f_steps,
-                "error_vs_fp64": _err(C2, ref), "kernel": "ffma_sgemm_kernel (tile 1: 128x128, packed FMA)"}
+                "error_vs_fp64": _err(C2, ref), "kernel": "ffma_sgemm_kernel (tile 1: 128x128, packed FMA)",
+                "kernel_ms": statistics.mean(f_kern)}
         del C2
     del ref
 
@@ -402,6 +411,8 @@ def run_ours(args) -> None:
     assert torch.equal(dC[(args.steps - 1) % 2], C)  # same inputs, same result
 
     peaks = _peaks()
+    fp32 = hb.fp32_peak(packed=True, iters=200000)  # measured FP32 SIMT roof, this device
+    fp32_scalar = hb.fp32_peak(packed=False, iters=200000)
     avg_kernel_ms = statistics.mean(kern_ms)
     if split:
         prods = PRODUCTS[variant]
@@ -418,16 +429,10 @@ def run_ours(args) -> None:
                 "effective_fp32_tflops_of_kernel": flops / (avg_kernel_ms * 1e-3) / 1e12}
         launches = args.steps * (3 + (2 if "scaled" in variant else 0))
     else:
-        achieved = flops / (avg_kernel_ms * 1e-3) / 1e12
-        sm_max = clocks.get("sm_max_mhz") or peaks["sm_max_mhz"]
-        peak_fp32 = SMS * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
-        roof = {"bound": "fp32_simt", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
-                "frac": achieved / peak_fp32, "traffic": _profile_traffic(f"ffma_sgemm_n{n}"),
-                "kernel": "ffma_sgemm_kernel", "algorithmic_flops_per_launch": flops,
-                "flops_note": f"derived peak: {SMS} SM x {FP32_LANES_PER_SM} FP32 lanes x 2 x "
-                              f"{sm_max:.0f} MHz (no measured FP32 peak exists)",
-                "kernel_ms": avg_kernel_ms}
+        roof = _ffma_roofline(statistics.mean(kern_ms), flops, fp32, n)
         launches = args.steps
+    if ffma is not None:
+        ffma["roofline"] = _ffma_roofline(ffma.pop("kernel_ms"), flops, fp32, n)
 
     line = {
         "metric": METRIC,
@@ -448,16 +453,89 @@ def run_ours(args) -> None:
         "roofline": roof,
         "clocks": clocks,
     }
+    line["fp32_peak_measured"] = {
+        "packed_ffma2_tflops": fp32["tflops"], "scalar_ffma_tflops": fp32_scalar["tflops"],
+        "probe": "hbsg_fp32_peak_probe: 8 independent FMA chains per thread, 4 CTAs x 256 "
+                 "threads per SM, best of 5 launches (CUDA events)",
+        "derived_tflops_at_sm_max": SMS * FP32_LANES_PER_SM * 2 *
+        (clocks.get("sm_max_mhz") or peaks["sm_max_mhz"]) * 1e6 / 1e12}
     if ffma is not None:
         line["ffma"] = ffma
         line["speedup_vs_ffma"] = value / ffma["value"]
         line["error_ratio_vs_ffma"] = err["rel_fro"] / ffma["error_vs_fp64"]["rel_fro"]
+    if not args.no_legs:
+        del A, B, C, wsp, dA, dB, dC, hA, hB, hC
+        torch.cuda.empty_cache()
+        line["configs"] = _config_legs(hb, peaks, fp32["tflops"], value,
+                                       ffma["value"] if ffma else None)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
+
+
+def _ffma_roofline(kernel_ms: float, flops: float, fp32: dict, n: int) -> dict:
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    return {"bound": "fp32_simt", "achieved": achieved, "peak": fp32["tflops"],
+            "unit": "TFLOP/s", "frac": achieved / fp32["tflops"],
+            "traffic": _profile_traffic(f"ffma_sgemm_n{n}"), "kernel": "ffma_sgemm_kernel",
+            "algorithmic_flops_per_launch": flops, "kernel_ms": kernel_ms,
+            "flops_note": "2*N^3 FP32 flops per launch; peak = the FP32 SIMT probe "
+                          "(packed __ffma2_rn, the instruction the kernel issues) measured "
+                          "on this device in this run"}
+
+
+# BASELINE configurations measured beside the headline: the uneven grouped
+# batch (512 problems) and the two awkward shapes, each one named case of the
+# sweep driver (seeded device inputs larger than L2; error vs FP64).
+LEGS = [
+    ("grouped_512_bf16x6", "GROUPED_512__SEED_0__V_bf16x6", 6),
+    ("grouped_512_ffma", "GROUPED_512__SEED_0__V_ffma", 0),
+    ("tallk_256x256x1048576_bf16x6", "M_256__N_256__K_1048576__V_bf16x6", 6),
+    ("tallk_256x256x1048576_bf16x3", "M_256__N_256__K_1048576__V_bf16x3", 3),
+    ("tallm_65536x64x4096_bf16x6", "M_65536__N_64__K_4096__V_bf16x6", 6),
+    ("tallm_65536x64x4096_bf16x3", "M_65536__N_64__K_4096__V_bf16x3", 3),
+    ("tallm_65536x64x4096_ffma", "M_65536__N_64__K_4096__V_ffma", 0),
+]
+
+
+def _config_legs(hb, peaks: dict, fp32_tflops: float, single_x6: float, single_ffma) -> dict:
+    """Each leg: effective TFLOP/s of the whole step (split passes included),
+    its error vs FP64, and the fraction of its roof: the lower of the compute
+    roof (BF16 burst / products, or the measured FP32 SIMT roof) and the HBM
+    roof (measured copy bandwidth x the step's algorithmic flop per byte:
+    2*M*N*K over 4*(M*K + K*N + M*N) bytes, summed over problems)."""
+    import torch
+
+    from hb_hammerbench_b200 import sweep
+    out = {}
+    for key, case, prods in LEGS:
+        r = sweep.run_case(case, steps=5, warmup=3)
+        c = sweep.parse_case(case)
+        if "GROUPED" in c:
+            dims = sweep.grouped_dims(c["GROUPED"], c.get("SEED", 0))
+        else:
+            dims = [(c["M"], c["N"], c["K"])]
+        fl = float(sum(2.0 * m * n * k for m, n, k in dims))
+        by = float(sum(4.0 * (m * k + k * n + m * n) for m, n, k in dims))
+        compute = peaks["bf16_tflops"] / prods if prods else fp32_tflops
+        hbm = peaks["hbm_gbs"] * 1e9 * (fl / by) / 1e12
+        roof = min(compute, hbm)
+        leg = {"case": case, "value": r["tflops"], "unit": "TFLOP/s", "ms_per_step": r["ms"],
+               "error_vs_fp64": r["error_vs_fp64"],
+               "roofline": {"bound": "hbm" if hbm < compute else ("tensor" if prods else "fp32_simt"),
+                            "roof_tflops": roof, "compute_roof_tflops": compute,
+                            "hbm_roof_tflops": hbm, "frac": r["tflops"] / roof,
+                            "algorithmic_bytes": by}}
+        if "GROUPED" in c:
+            single = single_x6 if prods else single_ffma
+            if single:
+                leg["ratio_to_single_8192"] = r["tflops"] / single
+        out[key] = leg
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -471,6 +549,8 @@ def main():
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FFMA comparison run")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the grouped and awkward-shape configuration legs")
     ap.add_argument("--profile", action="store_true",
                     help="timed steps only (no error check, e2e or CPU baseline): for ncu")
     args = ap.parse_args()

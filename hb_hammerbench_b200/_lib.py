@@ -49,7 +49,7 @@ class TileInfo(ctypes.Structure):
     """struct hbsg_tile_info"""
     _fields_ = [("variant_class", ctypes.c_int), ("bm", ctypes.c_int), ("bn", ctypes.c_int),
                 ("bk", ctypes.c_int), ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_int),
-                ("parts", ctypes.c_int)]
+                ("parts", ctypes.c_int), ("fused", ctypes.c_int)]
 
 
 class SplitLayout(ctypes.Structure):
@@ -81,6 +81,7 @@ SIGNATURES = {
     "hbsg_gemm_ex": (_I, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _I,
                           ctypes.POINTER(Config), _P, _SZ, _P]),
     "hbsg_gemm_workspace_size": (_SZ, [_I, _I, _I, _I, ctypes.POINTER(Config)]),
+    "hbsg_gemm_workspace_size_ex": (_SZ, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Config)]),
     "hbsg_get_split_layout": (_I, [_I, _I, _I, _I, ctypes.POINTER(SplitLayout)]),
     "hbsg_gemm_noalloc": (_I, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _I, _P]),
     "hbsg_grouped_workspace_size": (_SZ, [_I, ctypes.POINTER(Problem), _I, ctypes.POINTER(Config)]),
@@ -94,6 +95,7 @@ SIGNATURES = {
     "hbsg_strerror": (ctypes.c_char_p, [_I]),
     "hbsg_check_device": (_I, [_P]),
     "hbsg_debug_timeout_probe": (_I, [_P, _SZ, _P]),
+    "hbsg_fp32_peak_probe": (_I, [_I, _I, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "hbsg_version": (_I, []),
 }
 

@@ -98,6 +98,20 @@ __global__ void __launch_bounds__(256) split_b_kernel(const float* __restrict__ 
   split_b_block<P, SCALED>(B, ldb, K, N, Kp, Bp, colmax, blockIdx.y * 64, blockIdx.x * 64, tile);
 }
 
+cudaError_t maxabs_rows(const float* A, long lda, int M, int K, uint32_t* rowmax, cudaStream_t st) {
+  if (M > 0) row_maxabs_kernel<<<(M + 7) / 8, 256, 0, st>>>(A, lda, M, K, rowmax);
+  return cudaGetLastError();
+}
+
+cudaError_t maxabs_cols(const float* B, long ldb, int K, int N, uint32_t* colmax, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(colmax, 0, sizeof(uint32_t) * N, st);
+  if (e != cudaSuccess) return e;
+  const int kpb = 256;
+  dim3 g((N + 255) / 256, (K + kpb - 1) / kpb);
+  if (K > 0 && N > 0) col_maxabs_kernel<<<g, 256, 0, st>>>(B, ldb, K, N, kpb, colmax);
+  return cudaGetLastError();
+}
+
 static int grid_for(long work, int per_block, int sms) {
   long b = (work + per_block - 1) / per_block;
   const long cap = (long)sms * 8;

@@ -1,0 +1,457 @@
+// Split-BF16 tensor-core GEMM body with the FP32 -> BF16 split fused in
+// (tcgen05 cta_group::2, CTA pairs, sm_100a).
+//
+// The unfused path writes the BF16 parts of both operands to HBM in a split
+// pass and the product kernel reads them back: for an operand element that is
+// 4 bytes read + 2*P written + 2*P read again, against the 4 bytes the
+// product needs. Here the product kernel reads the FP32 operands itself:
+// converter warps load FP32 A rows and B columns with coalesced global loads
+// one k-tile ahead, split every value into P parts (exactly the split pass's
+// arithmetic: hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid)) and
+// write them into the shared-memory stage in the layout the TMA produced
+// before (K-major rows of 32 bf16 = 64 bytes, 64-byte swizzle: the 16-byte
+// chunk c of row r lands at chunk c ^ ((r >> 1) & 3)). The MMA issuer and the
+// epilogue are those of the pair kernel (tc_kernel2.cuh): same products, same
+// order, same TMEM drains, so the result is bit-identical to the unfused
+// kernels with the same drain interval.
+//
+// Why CTA pairs: the tensor core's shared-memory operand reads per MMA flop
+// are lowest for the 256 x 256 pair tile (each SM holds 128 A rows and 128 B
+// columns: ~64 of the 128 bytes/clock an SM's shared memory moves). The
+// converters' part writes add ~32 bytes/clock (6-product form), which still
+// fits; on a single-CTA 128 x 256 tile the MMA alone reads ~96 bytes/clock
+// and the writes would not fit.
+//
+// CTA (512 threads, 16 warps, one CTA per SM, clusters of two):
+//   warp 0       TMEM allocation; lane 0 of the leader CTA issues the MMAs
+//   warps 1-7    converters (this CTA's 128 A rows and BN/2 B columns)
+//   warps 8-15   epilogue (TMEM lane quadrant warp % 4, column half)
+// Register split (setmaxnreg): warpgroups 0-1 (issuer, converters) 104
+// registers per thread, warpgroups 2-3 (epilogue, BN/2 FP32 sums per thread)
+// 152: 2 x 128 x 104 + 2 x 128 x 152 = 65536, the block's launch allotment
+// (512 threads x 128). ptxas reports no spills for any instantiation at this
+// split (it spilled at 80/176, 88/168 and 96/160).
+// Every wait is bounded as in the other tensor-core bodies; no TMA is used.
+#pragma once
+
+#include "split_kernel.cuh"
+#include "tc_kernel2.cuh"
+
+namespace hbsg {
+
+static constexpr int kFusedThreads = 512;
+static constexpr int kConvWarps = 7;
+static constexpr int kConvThreads = kConvWarps * 32;
+static constexpr int kRegsLow = 104;   // warpgroups 0-1
+static constexpr int kRegsHigh = 152;  // warpgroups 2-3
+static_assert(2 * 128 * kRegsLow + 2 * 128 * kRegsHigh == 65536, "register split");
+
+// mbarrier probe with cluster-scope acquire: the converters of the peer CTA
+// arrive on the leader's stage barrier with release at cluster scope.
+HBSG_DEV bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+HBSG_DEV bool wait_bounded_cluster(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                   unsigned long long limit_ns) {
+  if (mbar_try_wait_cluster(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t i = 0;; ++i) {
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (globaltimer() - t0 > limit_ns) {
+        *abort_flag = 1;
+        atomicExch(&g_device_error, (int)HBSG_ERR_DEVICE_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+
+// Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).
+HBSG_DEV void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+template <int N>
+HBSG_DEV void regs_dec() {
+  asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(N));
+}
+template <int N>
+HBSG_DEV void regs_inc() {
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(N));
+}
+
+HBSG_DEV float ldg_stream(const float* p) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+HBSG_DEV float4 ldg_stream4(const float* p) {
+  float4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p));
+  return v;
+}
+
+HBSG_DEV void st_shared16(uint32_t addr, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y),
+               "r"(v.z), "r"(v.w)
+               : "memory");
+}
+
+HBSG_DEV uint32_t bf162_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t*>(&h); }
+
+// 32 lanes x 16 columns of 32-bit TMEM into 16 registers per thread.
+HBSG_DEV void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Splits 8 consecutive-k values of one row (A) or column (B) into P packed
+// 16-byte chunks, part 0 = hi: the split pass's arithmetic (split_value in
+// split_kernel.cuh), two values per conversion instruction.
+template <int P, bool SCALED>
+HBSG_DEV void split8(float (&x)[8], int e, uint4 (&out)[P]) {
+  if constexpr (SCALED) {
+    if (e != 0) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) x[i] = ldexpf(x[i], -e);
+    }
+  }
+  uint32_t h[4], m[4], l[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const __nv_bfloat162 hb = __floats2bfloat162_rn(x[2 * j], x[2 * j + 1]);
+    const float2 hf = __bfloat1622float2(hb);
+    const float r0 = x[2 * j] - hf.x;
+    const float r1 = x[2 * j + 1] - hf.y;
+    const __nv_bfloat162 mb = __floats2bfloat162_rn(r0, r1);
+    h[j] = bf162_bits(hb);
+    m[j] = bf162_bits(mb);
+    if constexpr (P == 3) {
+      const float2 mf = __bfloat1622float2(mb);
+      l[j] = bf162_bits(__floats2bfloat162_rn(r0 - mf.x, r1 - mf.y));
+    }
+  }
+  out[0] = make_uint4(h[0], h[1], h[2], h[3]);
+  out[1] = make_uint4(m[0], m[1], m[2], m[3]);
+  if constexpr (P == 3) out[2] = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+template <int P, int BN, int STAGES>
+struct TcFusedShape {
+  static constexpr int kHalf = BN / 2;                  // B columns per CTA
+  static constexpr int kABytes = kBM * kBK * 2;         // 128 rows of one part
+  static constexpr int kBBytes = kHalf * kBK * 2;       // this CTA's B columns, one part
+  static constexpr int kStageBytes = P * (kABytes + kBBytes);
+  static constexpr int kAllocCols = 2 * BN <= 32 ? 32 : 2 * BN <= 64 ? 64 : 2 * BN <= 128 ? 128 : 2 * BN <= 256 ? 256 : 512;
+  static constexpr int kBarBytes = 8 * (2 * STAGES + 4) + 16;
+  static constexpr int kColExpBytes = 8 * 4 * (BN / 2);
+  static constexpr int kSmemBytes = 1024 + STAGES * kStageBytes + kBarBytes + kColExpBytes;
+  // converter work per k-tile: 8-element units (one row of A or column of B,
+  // 8 consecutive k); A units first: unit u < kAUnits is row u / 4, chunk u % 4
+  static constexpr int kAUnits = kBM * 4;
+  static constexpr int kBUnits = kHalf * 4;
+  static constexpr int kUnits = kAUnits + kBUnits;
+  static constexpr int kUnitsPerThread = (kUnits + kConvThreads - 1) / kConvThreads;
+  static_assert(kSmemBytes <= 232448, "shared memory");
+  static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256, "pair UMMA N");
+  static_assert(kBBytes % 512 == 0, "B part base keeps the 512-byte swizzle alignment");
+  static_assert(kAUnits % 32 == 0, "a warp's units are all A or all B");
+};
+
+// Byte offset of the 16-byte chunk c (8 bf16) of row r in a part tile of
+// 64-byte rows with the 64-byte swizzle (address bits 4-5 ^= bits 7-8).
+HBSG_DEV uint32_t sw64_offset(int r, int c) {
+  return (uint32_t)(r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
+}
+
+template <int P, int BN, int STAGES, bool SCALED, bool VEC, class Tiles>
+__device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& run) {
+  using S = TcFusedShape<P, BN, STAGES>;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* smem = smem_raw + (base - raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * S::kStageBytes);
+  uint64_t* full = bars;                     // leader: both CTAs' converters filled the stage
+  uint64_t* empty = bars + STAGES;           // each CTA: the stage is free again
+  uint64_t* tfull = bars + 2 * STAGES;       // each CTA: accumulator buffer ready
+  uint64_t* tempty = bars + 2 * STAGES + 2;  // leader: both CTAs drained the buffer
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* col_exp = reinterpret_cast<int*>(smem + STAGES * S::kStageBytes + S::kBarBytes);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int pair = blockIdx.x >> 1;
+  const int pairs = gridDim.x >> 1;
+  const int num_tiles = tiles.count();
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 2 * kConvWarps);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 16);
+    }
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(S::kAllocCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n");
+  }
+  tc_fence_before();
+  cluster_sync();  // barriers of both CTAs initialised, TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const unsigned long long lim = run.wait_limit_ns;
+
+  if (warp < 8) {
+    regs_dec<kRegsLow>();
+  } else {
+    regs_inc<kRegsHigh>();
+  }
+
+  if (warp == 0) {
+    // ---------------- MMA issuer (leader CTA only) ----------------
+    if (leader && lane == 0) {
+      // full-width MMAs: each CTA holds a fixed half of the BN columns, so the
+      // instruction's N cannot be trimmed (padding columns are zeros)
+      constexpr uint32_t idesc = f16_idesc(2 * kBM, BN);
+      uint32_t it = 0, ch = 0;
+      bool ok = true;
+      for (int t = pair; t < num_tiles && ok; t += pairs) {
+        const TileWork w = tiles.get(t);
+        const int KT = w.KT;
+        const int nchunks = (KT + run.chunk_ktiles - 1) / run.chunk_ktiles;
+        int kt = 0;
+        for (int c = 0; c < nchunks && ok; ++c, ++ch) {
+          const int buf = ch & 1;
+          if (!wait_bounded(&tempty[buf], ((ch >> 1) & 1) ^ 1, abort_flag, lim)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem_base + buf * BN;
+          const int kend = min(KT, kt + run.chunk_ktiles);
+          bool first = true;
+          for (; kt < kend; ++kt, ++it) {
+            const int s = it % STAGES;
+            if (!wait_bounded_cluster(&full[s], (it / STAGES) & 1, abort_flag, lim)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sa = base + s * S::kStageBytes;
+            const uint32_t sb = sa + P * S::kABytes;
+#pragma unroll
+            for (int ks = 0; ks < kBK / 16; ++ks) {
+#pragma unroll
+              for (int q = 0; q < Products<P>::n; ++q) {
+                const uint64_t ad = sw64_desc(sa + Products<P>::a(q) * S::kABytes + ks * 32);
+                const uint64_t bd = sw64_desc(sb + Products<P>::b(q) * S::kBBytes + ks * 32);
+                tc_mma_pair(d, ad, bd, idesc, first ? 0u : 1u);
+                first = false;
+              }
+            }
+            tc_commit_pair(&empty[s]);
+          }
+          if (ok) tc_commit_pair(&tfull[buf]);
+        }
+      }
+    }
+  } else if (warp < 8) {
+    // ---------------- converters (both CTAs) ----------------
+    constexpr int NU = S::kUnitsPerThread;
+    const int cid = threadIdx.x - 32;
+    const uint32_t full_leader0 = map_to_rank(smem_u32(&full[0]), 0);
+    float v[NU][8];
+    int ex[NU];
+#pragma unroll
+    for (int i = 0; i < NU; ++i) ex[i] = 0;
+
+    // Loads unit i of k-tile kt of work item w into v[i] (zeros outside the
+    // matrix and beyond K), and its row/column exponent (scaled forms).
+    auto load_units = [&](const TileWork& w, int kt) {
+      const int kb = (w.kt0 + kt) * kBK;
+#pragma unroll
+      for (int i = 0; i < NU; ++i) {
+        const int u = cid + i * kConvThreads;
+        if (u >= S::kUnits) continue;
+        if (u < S::kAUnits) {
+          const int m = w.m0 + kBM * (int)rank + (u >> 2);
+          const int k = kb + (u & 3) * 8;
+          if (m < w.M) {
+            const float* src = w.A + (long)m * w.lda + k;
+            if (VEC && k + 8 <= w.K) {
+              const float4 a0 = ldg_stream4(src);
+              const float4 a1 = ldg_stream4(src + 4);
+              v[i][0] = a0.x; v[i][1] = a0.y; v[i][2] = a0.z; v[i][3] = a0.w;
+              v[i][4] = a1.x; v[i][5] = a1.y; v[i][6] = a1.z; v[i][7] = a1.w;
+            } else {
+#pragma unroll
+              for (int j = 0; j < 8; ++j) v[i][j] = k + j < w.K ? ldg_stream(src + j) : 0.0f;
+            }
+            if constexpr (SCALED) ex[i] = exp_from_maxbits(w.rowmax[m]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[i][j] = 0.0f;
+          }
+        } else {
+          const int ub = u - S::kAUnits;
+          const int n = w.n0 + S::kHalf * (int)rank + ub % S::kHalf;
+          const int k = kb + (ub / S::kHalf) * 8;
+          if (n < w.N) {
+            const float* src = w.B + (long)k * w.ldb + n;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[i][j] = k + j < w.K ? ldg_stream(src + (long)j * w.ldb) : 0.0f;
+            if constexpr (SCALED) ex[i] = exp_from_maxbits(w.colmax[n]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[i][j] = 0.0f;
+          }
+        }
+      }
+    };
+
+    uint32_t it = 0;
+    bool ok = true;
+    if (pair < num_tiles) load_units(tiles.get(pair), 0);
+    for (int t = pair; t < num_tiles && ok; t += pairs) {
+      // the work item is re-derived here rather than carried over from the
+      // previous item's prefetch, so only one item's fields stay live
+      const TileWork w = tiles.get(t);
+      for (int kt = 0; kt < w.KT; ++kt, ++it) {
+        const int s = it % STAGES;
+        if (!wait_bounded(&empty[s], ((it / STAGES) & 1) ^ 1, abort_flag, lim)) {
+          ok = false;
+          break;
+        }
+        const uint32_t sa = base + s * S::kStageBytes;
+        const uint32_t sb = sa + P * S::kABytes;
+#pragma unroll
+        for (int i = 0; i < NU; ++i) {
+          const int u = cid + i * kConvThreads;
+          if (u >= S::kUnits) continue;
+          uint4 o[P];
+          split8<P, SCALED>(v[i], ex[i], o);
+          if (u < S::kAUnits) {
+            const uint32_t off = sw64_offset(u >> 2, u & 3);
+#pragma unroll
+            for (int p = 0; p < P; ++p) st_shared16(sa + p * S::kABytes + off, o[p]);
+          } else {
+            const int ub = u - S::kAUnits;
+            const uint32_t off = sw64_offset(ub % S::kHalf, ub / S::kHalf);
+#pragma unroll
+            for (int p = 0; p < P; ++p) st_shared16(sb + p * S::kBBytes + off, o[p]);
+          }
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          if (leader) mbar_arrive(&full[s]);
+          else mbar_arrive_remote(full_leader0 + 8u * s);
+        }
+        // the next k-tile's operands, possibly of the next work item: issued
+        // now, consumed one stage later
+        if (kt + 1 < w.KT) load_units(w, kt + 1);
+        else if (t + pairs < num_tiles) load_units(tiles.get(t + pairs), 0);
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 8..15, both CTAs) ----------------
+    const int q = warp & 3;
+    const int h = (warp - 8) >> 2;
+    constexpr int COLS = BN / 2;
+    uint32_t ch = 0;
+    bool ok = true;
+    const uint32_t tempty_leader0 = map_to_rank(smem_u32(&tempty[0]), 0);
+    for (int t = pair; t < num_tiles && ok; t += pairs) {
+      const TileWork w = tiles.get(t);
+      const int nchunks = (w.KT + run.chunk_ktiles - 1) / run.chunk_ktiles;
+      float sum[COLS];
+#pragma unroll
+      for (int i = 0; i < COLS; ++i) sum[i] = 0.0f;
+      for (int c = 0; c < nchunks; ++c, ++ch) {
+        const int buf = ch & 1;
+        int got = 0;
+        if (lane == 0) got = wait_bounded(&tfull[buf], (ch >> 1) & 1, abort_flag, lim);
+        got = __shfl_sync(0xffffffffu, got, 0);
+        if (!got) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + buf * BN + h * COLS;
+#pragma unroll
+        for (int j = 0; j < COLS / 16; ++j) {
+          float vv[16];
+          tmem_ld16(taddr + 16 * j, vv);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) sum[16 * j + i] += vv[i];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_remote(tempty_leader0 + 8u * buf);
+      }
+      if (!ok) break;
+      const int col0 = w.n0 + h * COLS;
+      int* wexp = col_exp + (warp - 8) * COLS;
+      if constexpr (SCALED) {
+        __syncwarp();
+#pragma unroll
+        for (int i = lane; i < COLS; i += 32)
+          wexp[i] = pow2_exp_of_bits(w.colmax[min(col0 + i, w.N - 1)]);
+        __syncwarp();
+      }
+      store_rows_transposed<COLS, SCALED>(sum, w, w.m0 + kBM * (int)rank + 32 * q, col0, lane,
+                                          wexp);
+    }
+  }
+
+  // Every role leaves its loop (normally or through bounded aborts). After an
+  // abort, give in-flight tensor-core work a bounded moment; then the pair
+  // synchronises and releases its tensor memory together.
+  __syncthreads();
+  if (*abort_flag) {
+    const unsigned long long t0 = globaltimer();
+    while (globaltimer() - t0 < 2000000ull) {
+    }
+  }
+  tc_fence_before();
+  cluster_sync();
+  if (warp == 0) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base),
+                 "r"(S::kAllocCols));
+  }
+}
+
+}  // namespace hbsg

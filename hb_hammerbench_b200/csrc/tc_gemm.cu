@@ -170,7 +170,7 @@ static cudaError_t launch_tc(const CUtensorMap& a, const CUtensorMap& b, const T
   auto k0 = tc_gemm_kernel<P, BN, STAGES, false>;
   auto k1 = tc_gemm_kernel<P, BN, STAGES, true>;
   auto k = scaled ? k1 : k0;
-  static uint32_t m0 = 0, m1 = 0;
+  static uint64_t m0 = 0, m1 = 0;
   if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, scaled ? &m1 : &m0))
     return cudaErrorInvalidValue;
   k<<<grid, S::kThreads, S::kSmemBytes, st>>>(a, b, p, run);
@@ -188,7 +188,7 @@ static cudaError_t launch_tc_pair(const CUtensorMap& a, const CUtensorMap& b, co
   auto k0 = tc_pair_kernel<P, BN, STAGES, false>;
   auto k1 = tc_pair_kernel<P, BN, STAGES, true>;
   auto k = scaled ? k1 : k0;
-  static uint32_t m0 = 0, m1 = 0;
+  static uint64_t m0 = 0, m1 = 0;
   if (!set_smem_once(reinterpret_cast<const void*>(k), S::kSmemBytes, scaled ? &m1 : &m0))
     return cudaErrorInvalidValue;
   k<<<grid, 320, S::kSmemBytes, st>>>(a, b, p, run);
@@ -255,6 +255,9 @@ bool tc_make_parts_map(void* map, const void* parts, int P, int rows, int Kp, in
 // (tile, slice) work items to fill the concurrent slots when the output alone
 // has fewer than half as many tiles as slots, each slice keeping >= 8
 // k-tiles; `requested` > 0 overrides. Normalised so that no slice is empty.
+// Automatic slices shorter than this many k-tiles are not used (see tc_pick_tile).
+static constexpr int kMinSliceKtiles = 16;
+
 static int slices_for(long tiles, int KT, int slots, int requested, int* kt_per_split) {
   int s = requested;
   if (s <= 0) {
@@ -272,6 +275,18 @@ static int ktiles_of(int K) {
   return KT > 0 ? KT : 1;
 }
 
+int tc_slices(long tiles, int K, int slots, int requested, int* kt_per_split) {
+  const int KT = ktiles_of(K);
+  int per = KT;
+  int s = slices_for(tiles, KT, slots, requested, &per);
+  if (requested <= 0 && s > 1 && per < kMinSliceKtiles) {
+    s = 1;
+    per = KT;
+  }
+  if (kt_per_split) *kt_per_split = per;
+  return s;
+}
+
 // Tile shape for an M x N x K product: scored on the work items it yields
 // after K slicing (so a tall-K problem with a small output takes the wide,
 // efficient tile and fills the GPU with slices rather than narrow tiles),
@@ -280,8 +295,6 @@ static int ktiles_of(int K) {
 // kMinSliceKtiles are not counted: their FP32 partials, the reduction and
 // the pipeline refill outweigh the wider tile (measured at 1024^3, 1000^3
 // and 128x128x65536: 15-30 % slower than unsliced narrow tiles).
-static constexpr int kMinSliceKtiles = 16;
-
 int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits) {
   const int KT = ktiles_of(K);
   int best = -1;
@@ -311,11 +324,15 @@ int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits) 
   return best;
 }
 
+// K slices the launch uses: the same rule the tile choice scored (automatic
+// slices shorter than kMinSliceKtiles are dropped for one unsliced pass), so
+// the schedule that runs is the one that was chosen, and the workspace holds
+// no partial buffer for slices that never run.
 int tc_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
   const TcEntry& e = kTcTiles[idx];
   const int tbm = e.pair ? 2 * kBM : kBM;
   const long tiles = (long)((M + tbm - 1) / tbm) * ((N + e.bn - 1) / e.bn);
-  return slices_for(tiles, ktiles_of(K), e.pair ? sms / 2 : sms, requested, kt_per_split);
+  return tc_slices(tiles, K, e.pair ? sms / 2 : sms, requested, kt_per_split);
 }
 
 cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,

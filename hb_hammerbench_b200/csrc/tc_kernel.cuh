@@ -220,6 +220,12 @@ struct TileWork {
   int KT;   // k-tiles in this work item
   const uint32_t* rowmax;  // scaled forms only
   const uint32_t* colmax;
+  // FP32 operands, read by the fused-split body only (tc_fused.cuh): A is
+  // M x K (row stride lda), B is K x N (row stride ldb)
+  const float* A = nullptr;
+  const float* B = nullptr;
+  long lda = 0, ldb = 0;
+  int K = 0;
 };
 
 // Settings shared by every tile of a launch.

@@ -117,7 +117,8 @@ def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, varian
     v = _variant(variant)
     cfgp = _config(config)
     with torch.cuda.device(a.device):
-        need = int(lib().hbsg_gemm_workspace_size(m, n, k, v, cfgp))
+        need = int(lib().hbsg_gemm_workspace_size_ex(int(trans_a), int(trans_b), m, n, k, v,
+                                                     cfgp))
         ws = _workspace(need, a.device, workspace)
         st = lib().hbsg_gemm_ex(int(trans_a), int(trans_b), m, n, k, _ptr(a), a.stride(0),
                                 _ptr(b), b.stride(0), _ptr(c), c.stride(0), v, cfgp,
@@ -218,9 +219,36 @@ def tiles() -> list[dict]:
         out.append({"tile": t, "family": "ffma" if info.variant_class == 0 else "bf16",
                     "bm": info.bm, "bn": info.bn, "bk": info.bk,
                     "threads": info.threads, "smem_bytes": info.smem_bytes,
-                    "parts": info.parts})
+                    "parts": info.parts, "fused": bool(info.fused)})
     return out
 
 
 def check_device() -> None:
     check(lib().hbsg_check_device(_stream()), "device check")
+
+
+def fp32_peak(packed: bool = True, iters: int = 4096, repeats: int = 5) -> dict:
+    """Measured FP32 SIMT roof of the current device: the probe kernel of
+    independent FMA chains (hbsg_fp32_peak_probe) timed with CUDA events on
+    the current stream, best of `repeats` launches after one warm-up launch.
+    Returns {"tflops": ..., "ms": ..., "flops": ...}."""
+    sink = torch.zeros(1, device="cuda")
+    flops = ctypes.c_double()
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        check(lib().hbsg_fp32_peak_probe(int(packed), iters, _ptr(sink), ctypes.byref(flops),
+                                         _stream()), "hbsg_fp32_peak_probe")
+    launch()
+    best = None
+    for _ in range(repeats):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return {"tflops": flops.value / (best * 1e-3) / 1e12, "ms": best, "flops": flops.value}
+

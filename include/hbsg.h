@@ -82,6 +82,8 @@ typedef struct hbsg_tile_info {
     int smem_bytes;    /* dynamic shared memory per CTA */
     int parts;         /* split-BF16 family: BF16 parts per operand (3 -> BF16X6 forms,
                           2 -> BF16X3 forms); 0 for the FFMA family */
+    int fused;         /* 1: the FP32 -> BF16 split runs inside the product kernel (no
+                          split pass, no parts in the workspace; row-major operands only) */
 } hbsg_tile_info;
 
 /* ---------------------------------------------------------------------------
@@ -129,8 +131,16 @@ int hbsg_gemm_ex(int trans_a, int trans_b, int m, int n, int k,
                  float* c, int64_t ldc, int variant, const hbsg_config* cfg,
                  void* workspace, size_t workspace_bytes, hbsg_stream_t stream);
 
+/* Workspace bytes for hbsg_gemm / hbsg_gemm_ex on the current device. The
+ * split-BF16 schedule, and so its K-slice partial buffer, depends on the
+ * device's SM count: with no sm_100 device current the split-BF16 forms
+ * report 0 (and the product call itself returns HBSG_ERR_NO_DEVICE). */
 size_t hbsg_gemm_workspace_size(int m, int n, int k, int variant,
                                 const hbsg_config* cfg);
+/* The same for a call with transposed operands (the automatic schedule of a
+ * transposed call never uses a fused-split tile, so its size can differ). */
+size_t hbsg_gemm_workspace_size_ex(int trans_a, int trans_b, int m, int n, int k, int variant,
+                                   const hbsg_config* cfg);
 
 /* Where the split-BF16 path keeps the operand parts inside its workspace
  * (byte offsets from the workspace start). Parts are BF16, K-major:
@@ -162,6 +172,12 @@ int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* o
  * problems' pointers: rerun it whenever the operand contents change, and
  * keep the workspace alive and untouched while the plan exists.
  * hbsg_gemm_grouped builds the tables and launches directly (no graph).
+ *
+ * Both hbsg_grouped_plan_create and hbsg_gemm_grouped write their tables into
+ * the workspace with blocking host-to-device copies that are not ordered
+ * after work on other streams: the workspace must be idle (every earlier
+ * launch that reads it, such as a previous hbsg_grouped_run on another
+ * stream, complete) when either is called.
  */
 typedef struct hbsg_problem {
     int m, n, k;
@@ -204,7 +220,9 @@ int hbsg_gemm_grouped(int count, const hbsg_problem* problems, int variant,
  *     hbsg_gemm).
  *   - The first call on each device looks up the array's device address
  *     (set-up, no allocation); make that first call before any stream
- *     capture begins.
+ *     capture begins. The address is kept for the process's life and does
+ *     not survive cudaDeviceReset: do not call this entry point on a device
+ *     after resetting it.
  *   - All calls on a device share the one array: calls that may overlap on
  *     the GPU (different streams without ordering between them) race on it
  *     and must be serialised by the caller. Nothing needs clearing between
@@ -235,6 +253,16 @@ int hbsg_check_device(hbsg_stream_t stream);
  * aligned) only backs the tensor maps; nothing is read or written. The next
  * hbsg_check_device reports the timeout. No reference counterpart. */
 int hbsg_debug_timeout_probe(void* workspace, size_t workspace_bytes, hbsg_stream_t stream);
+
+/* FP32 SIMT throughput probe (no reference counterpart): launches a kernel
+ * of independent fused multiply-add chains on every SM of the current device
+ * (packed != 0: the packed two-lane __ffma2_rn the FFMA kernel issues;
+ * 0: scalar FMA) for `iters` steps and stores in *flops_out the FP32 flops it
+ * performs. Time the launch on `stream` (CUDA events) to get the device's
+ * FP32 roof: the denominator of the FFMA kernel's roofline fraction. `sink`
+ * is one device float the kernel writes only on an impossible result. */
+int hbsg_fp32_peak_probe(int packed, int iters, float* sink, double* flops_out,
+                         hbsg_stream_t stream);
 
 /* ABI version (major * 100 + minor). */
 int hbsg_version(void);
