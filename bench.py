@@ -268,11 +268,23 @@ def run_ours(args) -> None:
     A = torch.rand((n, n), device=dev, generator=g) * 2 - 1
     B = torch.rand((n, n), device=dev, generator=g) * 2 - 1
     C = torch.empty((n, n), device=dev)
-    wsz = hb.gemm_workspace_size(n, n, n, variant)
+    # the schedule every call below runs: the autotuner's choice for this
+    # shape class when the package ships one, else the library heuristic
+    sched = hb.resolve_config(n, n, n, variant, False, None) or {}
+    tile_info = {t["tile"]: t for t in hb.tiles()}
+    if split:
+        tile = sched.get("tile") or 0
+        fused = bool(tile and tile_info[tile]["fused"])
+    else:
+        fused = False
+    wsz = hb.gemm_workspace_size(n, n, n, variant, config=sched or None)
     wsp = torch.empty(max(wsz, 256), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
-    split_only = {"flags": _lib.FLAG_SPLIT_ONLY}
-    presplit = {"flags": _lib.FLAG_PRESPLIT_A | _lib.FLAG_PRESPLIT_B}
+    # split-BF16 step = split-only call (the split passes; for a fused-split
+    # schedule only the scaled forms' row/column maxima) + pre-split call (the
+    # tensor-core product), so the product kernel can be timed on its own
+    split_only = {**sched, "flags": _lib.FLAG_SPLIT_ONLY}
+    presplit = {**sched, "flags": _lib.FLAG_PRESPLIT_A | _lib.FLAG_PRESPLIT_B}
 
     def barrier():
         if ws > 1:
@@ -387,7 +399,7 @@ def run_ours(args) -> None:
             stream.wait_event(in_done[i])
             if i >= 2:
                 stream.wait_event(out_done[i - 2])  # dC[b] already copied out
-            hb.gemm(dA[b], dB[b], dC[b], variant=variant, workspace=wsp)
+            hb.gemm(dA[b], dB[b], dC[b], variant=variant, workspace=wsp, config=sched or None)
             cmp_done[i].record(stream)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(cmp_done[i])
@@ -418,16 +430,19 @@ def run_ours(args) -> None:
         prods = PRODUCTS[variant]
         mma_flops = prods * flops
         achieved = mma_flops / (avg_kernel_ms * 1e-3) / 1e12
-        traffic = _profile_traffic(f"tc_gemm_{variant}_n{n}")
+        kname = "tc_fused_kernel" if fused else "tc_gemm_kernel"
+        traffic = _profile_traffic(f"{kname[:-7]}_{variant}_n{n}")
         roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
                 "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
-                "kernel": "tc_gemm_kernel", "algorithmic_flops_per_launch": mma_flops,
+                "kernel": kname, "algorithmic_flops_per_launch": mma_flops,
                 "flops_note": f"{prods} BF16 products x 2*N^3 executed on the tensor cores per launch; "
                               f"peak = {peaks['source']} cuBLAS bf16 burst",
                 "frac_of_sustained": achieved / peaks["bf16_tflops_sustained"],
                 "kernel_ms": avg_kernel_ms,
                 "effective_fp32_tflops_of_kernel": flops / (avg_kernel_ms * 1e-3) / 1e12}
-        launches = args.steps * (3 + (2 if "scaled" in variant else 0))
+        # per step: split passes (A, B; none when fused), row/column maxima
+        # (scaled forms), the product kernel
+        launches = args.steps * ((0 if fused else 2) + (2 if "scaled" in variant else 0) + 1)
     else:
         roof = _ffma_roofline(statistics.mean(kern_ms), flops, fp32, n)
         launches = args.steps
@@ -441,7 +456,8 @@ def run_ours(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded i.i.d. U[-1,1) float32, built on the device",
         "config": {"workload": f"sgemm M=N=K={n} fp32 row-major, variant {variant}",
-                   "m": n, "n": n, "k": n, "variant": variant,
+                   "m": n, "n": n, "k": n, "variant": variant, "schedule": sched or "heuristic",
+                   "fused_split": fused,
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single",
                    "l2": "inputs (268 MB each) larger than L2; no flush"},
         "error_vs_fp64": {**err, "reference": "FP64 product of the same inputs (torch float64 "

@@ -16,6 +16,14 @@ sweep (apps/legacy/gemm/sgemm_512/tests.mk:1-6), run by hand.
 Shape class: the variant and the power-of-two bucket (ceil log2) of M, N
 and K. Cache file: $HBSG_AUTOTUNE_CACHE, else
 ~/.cache/hb_hammerbench_b200/autotune.json (written atomically).
+
+Defaults: the package ships the table this tuner produced on a B200
+(tuned_b200.json, regenerated with `python -m hb_hammerbench_b200.autotune
+--ship`). lookup() answers from the user cache first, then from that table, so
+the host interface (sgemm.gemm, sgemm.GroupedPlan) runs the tuner's choice
+for every tuned shape class when the caller passes no schedule; shapes of no
+tuned class keep the C library's heuristic. HBSG_AUTOTUNE=0 turns the lookup
+off.
 """
 from __future__ import annotations
 
@@ -28,6 +36,25 @@ import threading
 
 _lock = threading.Lock()
 _mem: dict | None = None
+_shipped: dict | None = None
+_last_entry: dict | None = None  # the table entry of the latest tune / tune_grouped
+
+SHIPPED_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_b200.json")
+
+
+def enabled() -> bool:
+    return os.environ.get("HBSG_AUTOTUNE", "1") != "0"
+
+
+def _load_shipped() -> dict:
+    global _shipped
+    if _shipped is None:
+        try:
+            with open(SHIPPED_PATH) as f:
+                _shipped = json.load(f)
+        except (OSError, ValueError):
+            _shipped = {}
+    return _shipped
 
 
 def cache_path() -> str:
@@ -74,18 +101,24 @@ def _store(key: str, entry: dict) -> None:
 
 
 def clear_memory_cache() -> None:
-    global _mem
+    global _mem, _shipped
     _mem = None
+    _shipped = None
+
+
+def _entry(key: str):
+    return _load().get(key) or _load_shipped().get(key)
 
 
 def lookup(m: int, n: int, k: int, variant: str) -> dict | None:
-    """Cached best schedule for the shape class, or None."""
-    e = _load().get(shape_key(m, n, k, variant))
+    """Best measured schedule for the shape class (user cache, then the
+    shipped table), or None."""
+    e = _entry(shape_key(m, n, k, variant))
     return dict(e["config"]) if e else None
 
 
 def lookup_grouped(dims, variant: str) -> dict | None:
-    e = _load().get(grouped_key(dims, variant))
+    e = _entry(grouped_key(dims, variant))
     return dict(e["config"]) if e else None
 
 
@@ -155,6 +188,8 @@ def tune(m: int, n: int, k: int, variant: str = "bf16x6", steps: int = 5,
     best = min(ok, key=lambda t: t["ms"])
     entry = {"config": best["config"], "ms": best["ms"], "shape": [m, n, k],
              "candidates": table}
+    global _last_entry
+    _last_entry = entry
     if store:
         _store(shape_key(m, n, k, variant), entry)
     return dict(best["config"])
@@ -183,7 +218,65 @@ def tune_grouped(As, Bs, variant: str = "bf16x6", steps: int = 3, store: bool = 
         raise RuntimeError("no candidate schedule ran")
     best = min(ok, key=lambda t: t["ms"])
     dims = [(a.shape[0], b.shape[1], a.shape[1]) for a, b in zip(As, Bs)]
+    entry = {"config": best["config"], "ms": best["ms"], "problems": len(dims),
+             "candidates": table}
+    global _last_entry
+    _last_entry = entry
     if store:
-        _store(grouped_key(dims, variant), {"config": best["config"], "ms": best["ms"],
-                                            "candidates": table})
+        _store(grouped_key(dims, variant), entry)
     return dict(best["config"])
+
+
+# Shape classes the shipped table covers: the benchmark's named
+# configurations (square sweep, the 8192^3 precision forms, the awkward
+# shapes, the uneven 512-problem batch).
+SHIP_SHAPES = [
+    ((1024, 1024, 1024), ("ffma", "bf16x6", "bf16x3")),
+    ((2048, 2048, 2048), ("ffma", "bf16x6", "bf16x3")),
+    ((4096, 4096, 4096), ("ffma", "bf16x6", "bf16x3")),
+    ((8192, 8192, 8192), ("ffma", "bf16x6", "bf16x3", "bf16x6_scaled", "bf16x3_scaled")),
+    ((256, 256, 1 << 20), ("ffma", "bf16x6", "bf16x3")),
+    ((65536, 64, 4096), ("ffma", "bf16x6", "bf16x3")),
+]
+SHIP_GROUPED = [(512, 0, ("ffma", "bf16x6", "bf16x3"))]
+
+
+def ship(path: str = SHIPPED_PATH, steps: int = 3) -> dict:
+    """Tune every shipped shape class on the current GPU and write the table
+    (with each candidate's measured time as evidence) to `path`."""
+    import torch
+
+    from . import sweep
+    out = {}
+    for (m, n, k), variants in SHIP_SHAPES:
+        for v in variants:
+            cfg = tune(m, n, k, v, steps=steps, max_candidates=64, store=False)
+            out[shape_key(m, n, k, v)] = _last_entry
+            print(json.dumps({"shape": [m, n, k], "variant": v, "config": cfg,
+                              "ms": _last_entry["ms"]}), flush=True)
+            torch.cuda.empty_cache()
+    for count, seed, variants in SHIP_GROUPED:
+        dims = sweep.grouped_dims(count, seed)
+        shapes = [(int(a), int(b), int(c)) for a, b, c in dims]
+        As, Bs = sweep._inputs(shapes, "uniform", seed, "cuda")
+        for v in variants:
+            cfg = tune_grouped(As, Bs, v, steps=steps, store=False)
+            out[grouped_key(shapes, v)] = _last_entry
+            print(json.dumps({"grouped": count, "variant": v, "config": cfg,
+                              "ms": _last_entry["ms"]}), flush=True)
+        del As, Bs
+        torch.cuda.empty_cache()
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="autotuner")
+    ap.add_argument("--ship", action="store_true", help="tune the shipped shape classes")
+    ap.add_argument("--out", default=SHIPPED_PATH)
+    ap.add_argument("--steps", type=int, default=3)
+    a = ap.parse_args()
+    if a.ship:
+        ship(a.out, a.steps)

@@ -31,7 +31,7 @@
 
 #include "ffma_kernel.cuh"
 #include "split_kernel.cuh"
-#include "tc_kernel.cuh"
+#include "tc_fused.cuh"
 
 namespace hbsg {
 
@@ -78,6 +78,11 @@ struct GTiles {  // tile source for the tensor-core body (split pass run beforeh
     w.KT = p.Kp / kBK;
     w.rowmax = p.rowmax;
     w.colmax = p.colmax;
+    w.A = p.A;
+    w.B = p.B;
+    w.lda = p.lda;
+    w.ldb = p.ldb;
+    w.K = p.K;
     return w;
   }
 };
@@ -85,6 +90,15 @@ struct GTiles {  // tile source for the tensor-core body (split pass run beforeh
 template <int P, int BN, int STAGES, bool SCALED>
 __global__ void __launch_bounds__(320, 1) tc_grouped_kernel(const GTiles tiles, const TcRun run) {
   tc_body<P, BN, STAGES, SCALED>(tiles, run);
+}
+
+// Fused-split form: CTA pairs over 256-row tiles, the split done by the
+// product kernel's converter warps (tc_fused.cuh); no split pass and no parts
+// in the workspace.
+template <int P, int BN, int STAGES, bool SCALED, bool VEC>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kFusedThreads, 1)
+    tc_grouped_fused_kernel(const GTiles tiles, const TcRun run) {
+  tc_fused_body<P, BN, STAGES, SCALED, VEC>(tiles, run);
 }
 
 // ---- inline split --------------------------------------------------------------
@@ -480,8 +494,9 @@ struct GroupedPlan {
   int variant;
   int count;
   bool inline_split;
-  int ffma_tile;  // index into the FFMA table, or -1
-  int tc_tile;    // index into the tensor-core table, or -1
+  int ffma_tile;   // index into the FFMA table, or -1
+  int tc_tile;     // index into the tensor-core table, or -1
+  int fused_tile;  // index into the fused table, or -1
   GLayout L;
   uint8_t* ws;
   int grid;
@@ -543,10 +558,11 @@ static GSets grouped_sets(int count, const hbsg_problem* pr, int variant, const 
 
 // Tile counts and job counts for a problem set (host arrays).
 static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, int bm, int bn,
-                              const GSets& sets) {
+                              const GSets& sets, bool fused = false) {
   const bool inline_split = sets.any_inline;
   GLayout L{};
   const bool split = variant != HBSG_FFMA;
+  const bool parts_in_hbm = split && !fused;
   const int P = split ? parts_of_v(variant) : 0;
   const bool scaled = split && scaled_of_v(variant);
   size_t parts = 0, maxes = 0, cmax = 0;
@@ -554,7 +570,7 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
     const hbsg_problem& q = pr[i];
     if (q.m <= 0 || q.n <= 0) continue;
     L.num_tiles += (long)((q.m + bm - 1) / bm) * ((q.n + bn - 1) / bn);
-    if (split) {
+    if (parts_in_hbm) {
       const int Kp = kp_of(q.k);
       parts += al((size_t)P * q.m * Kp * 2, 256) + al((size_t)P * q.n * Kp * 2, 256);
       if (sets.inl[i]) {
@@ -564,6 +580,8 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
         L.num_jobs_a += (units + 2047) / 2048;
         L.num_jobs_b += (long)((Kp + 63) / 64) * ((q.n + 63) / 64);
       }
+    }
+    if (split) {
       if (scaled) {
         maxes += al((size_t)q.m * 4, 256);
         cmax += al((size_t)q.n * 4, 256);
@@ -575,7 +593,7 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
   L.probs_off = 0;
   L.tiles_off = al(sizeof(GProblem) * (size_t)count, 256);
   L.maps_off = al(L.tiles_off + sizeof(int4) * (size_t)L.num_tiles, 256);
-  L.jobs_off = al(L.maps_off + (split ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
+  L.jobs_off = al(L.maps_off + (parts_in_hbm ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
   const long jobs = L.num_jobs_a + L.num_jobs_b + L.num_jobs_rmax + L.num_jobs_cmax;
   L.sync_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);
   L.sync_bytes = inline_split ? al(sizeof(int) * ((size_t)count + 1), 256) : 0;
@@ -587,11 +605,12 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
   return L;
 }
 
-static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* tc_idx, int* bm,
-                       int* bn) {
+static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* tc_idx,
+                       int* fused_idx, int* bm, int* bn) {
   const int nf = ffma_num_tiles();
   const int tile = cfg && cfg->tile > 0 ? cfg->tile - 1 : -1;
   hbsg_tile_info info;
+  *fused_idx = -1;
   if (variant == HBSG_FFMA) {
     int idx = tile >= 0 ? tile : 0;  // default: 128 x 128, packed FMA
     if (idx >= nf) return false;
@@ -604,6 +623,17 @@ static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* 
   }
   const int P = parts_of_v(variant);
   int idx = -1;
+  if (tile >= nf + tc_num_tiles()) {  // a fused-split tile
+    const int f = tile - nf - tc_num_tiles();
+    if (f >= fused_num_tiles() || fused_tile_parts(f) != P) return false;
+    fused_tile_info(f, &info);
+    *ffma_idx = -1;
+    *tc_idx = -1;
+    *fused_idx = f;
+    *bm = info.bm;
+    *bn = info.bn;
+    return true;
+  }
   if (tile >= 0) {
     idx = tile - nf;
     if (idx < 0 || idx >= tc_num_tiles() || tc_tile_parts(idx) != P || tc_tile_pair(idx))
@@ -668,6 +698,42 @@ static uint64_t g_tci_masks[sizeof(kGTcInline) / sizeof(kGTcInline[0])][2];
 static uint64_t g_ffma_masks[9][2];
 static uint64_t g_tc_masks[sizeof(kGTc) / sizeof(kGTc[0])][2];
 
+struct GFusedEntry {
+  int smem;
+  const void* k[4];  // [scaled * 2 + vec]
+};
+#define HBSG_GFUSED_ENTRY(P, BN, ST)                                                       \
+  GFusedEntry{TcFusedShape<P, BN, ST>::kSmemBytes,                                         \
+              {reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, false, false>), \
+               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, false, true>),  \
+               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, true, false>),  \
+               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, true, true>)}},
+static const GFusedEntry kGFused[] = {HBSG_FUSED_TILE_LIST(HBSG_GFUSED_ENTRY)};
+static constexpr int kNumGFused = sizeof(kGFused) / sizeof(kGFused[0]);
+static uint64_t g_fused_masks[kNumGFused][4];
+static int g_fused_regs[kNumGFused][4];
+
+// Co-resident clusters of two CTAs of a grouped fused kernel (0 if unknown).
+static int gfused_clusters(const void* k, int smem) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kFusedThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = 2;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 // Launches of one grouped product on `st` (no host synchronisation, no
 // allocation: capturable).
 static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
@@ -725,6 +791,21 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
   gt.maps = reinterpret_cast<const CUtensorMap*>(pl.ws + L.maps_off);
   gt.n = (int)L.num_tiles;
   TcRun run = pl.run;
+  if (pl.fused_tile >= 0) {
+    const int slot = (scaled ? 2 : 0) + (pl.vec ? 1 : 0);
+    const GFusedEntry& fe = kGFused[pl.fused_tile];
+    const void* k = fe.k[slot];
+    if (!set_smem_once(k, fe.smem, &g_fused_masks[pl.fused_tile][slot]))
+      return cudaErrorInvalidValue;
+    if (!fused_regs_ok(k, &g_fused_regs[pl.fused_tile][slot])) return cudaErrorInvalidConfiguration;
+    void* args[] = {&gt, &run};
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(pl.grid);
+    lc.blockDim = dim3(kFusedThreads);
+    lc.dynamicSmemBytes = fe.smem;
+    lc.stream = st;
+    return cudaLaunchKernelExC(&lc, k, args);
+  }
   if (pl.inline_split) {
     e = cudaMemsetAsync(pl.ws + L.sync_off, 0, L.sync_bytes, st);
     if (e != cudaSuccess) return e;
@@ -777,12 +858,16 @@ static int validate(int count, const hbsg_problem* pr, int variant) {
 static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const hbsg_config* cfg,
                       void* ws, size_t ws_bytes) {
   int bm = 0, bn = 0;
-  if (!tile_shape(pl->variant, cfg, &pl->ffma_tile, &pl->tc_tile, &bm, &bn))
+  if (!tile_shape(pl->variant, cfg, &pl->ffma_tile, &pl->tc_tile, &pl->fused_tile, &bm, &bn))
     return HBSG_ERR_UNSUPPORTED;
+  const bool fused = pl->fused_tile >= 0;
   pl->count = count;
-  const GSets sets = grouped_sets(count, pr, pl->variant, cfg);
+  hbsg_config no_inline{};
+  if (cfg) no_inline = *cfg;
+  no_inline.inline_split_pct = -1;  // fused plans split inside the product kernel already
+  const GSets sets = grouped_sets(count, pr, pl->variant, fused ? &no_inline : cfg);
   pl->inline_split = sets.any_inline;
-  pl->L = grouped_layout(count, pr, pl->variant, bm, bn, sets);
+  pl->L = grouped_layout(count, pr, pl->variant, bm, bn, sets, fused);
   const GLayout& L = pl->L;
   if (!ws || ws_bytes < L.total || (reinterpret_cast<uintptr_t>(ws) & 255)) return HBSG_ERR_WORKSPACE;
   pl->ws = static_cast<uint8_t*>(ws);
@@ -814,10 +899,12 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
           (reinterpret_cast<uintptr_t>(q.b) & 15))
         pl->vec = false;
       if (split) {
-        g.Ap = pl->ws + parts_cur;
-        parts_cur += al((size_t)P * q.m * g.Kp * 2, 256);
-        g.Bp = pl->ws + parts_cur;
-        parts_cur += al((size_t)P * q.n * g.Kp * 2, 256);
+        if (!fused) {
+          g.Ap = pl->ws + parts_cur;
+          parts_cur += al((size_t)P * q.m * g.Kp * 2, 256);
+          g.Bp = pl->ws + parts_cur;
+          parts_cur += al((size_t)P * q.n * g.Kp * 2, 256);
+        }
         if (scaled) {
           g.colmax = reinterpret_cast<uint32_t*>(pl->ws + cmax_cur);
           cmax_cur += al((size_t)q.n * 4, 256);
@@ -849,7 +936,7 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   std::vector<int4> jobs;
   std::vector<CUtensorMap> maps;
   if (split) {
-    {
+    if (!fused) {
       for (int i = 0; i < count; ++i) {  // A split jobs (problems split before the product)
         const GProblem& g = probs[i];
         if (g.M <= 0 || g.N <= 0 || sets.inl[i]) continue;
@@ -877,16 +964,18 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
           for (int k0 = 0; k0 < g.K; k0 += 256) jobs.push_back(make_int4(i, n0, k0, 0));
       }
     }
-    maps.resize(2 * (size_t)count);
-    for (int i = 0; i < count; ++i) {
-      const GProblem& g = probs[i];
-      if (g.M <= 0 || g.N <= 0) {
-        memset(&maps[2 * i], 0, 2 * sizeof(CUtensorMap));
-        continue;
+    if (!fused) {
+      maps.resize(2 * (size_t)count);
+      for (int i = 0; i < count; ++i) {
+        const GProblem& g = probs[i];
+        if (g.M <= 0 || g.N <= 0) {
+          memset(&maps[2 * i], 0, 2 * sizeof(CUtensorMap));
+          continue;
+        }
+        if (!tc_make_parts_map(&maps[2 * i], g.Ap, P, g.M, g.Kp, kBM) ||
+            !tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp, bn))
+          return HBSG_ERR_UNSUPPORTED;
       }
-      if (!tc_make_parts_map(&maps[2 * i], g.Ap, P, g.M, g.Kp, kBM) ||
-          !tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp, bn))
-        return HBSG_ERR_UNSUPPORTED;
     }
     pl->run.chunk_ktiles = tc_chunk_ktiles(P, cfg ? cfg->chunk_k : 0);
     pl->run.l2_ahead = tc_l2_ahead();
@@ -931,6 +1020,17 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   }
   if (e != cudaSuccess) return status_of(e);
 
+  if (fused) {
+    // CTA pairs: grid = 2 x min(tiles, co-resident clusters)
+    const int slot = (scaled ? 2 : 0) + (pl->vec ? 1 : 0);
+    const GFusedEntry& fe = kGFused[pl->fused_tile];
+    if (!set_smem_once(fe.k[slot], fe.smem, &g_fused_masks[pl->fused_tile][slot]))
+      return HBSG_ERR_LAUNCH;
+    int resident = gfused_clusters(fe.k[slot], fe.smem);
+    if (resident <= 0 || resident > sms / 2) resident = sms / 2;
+    pl->grid = (int)(2 * std::max<long>(1, std::min<long>(resident, L.num_tiles)));
+    return HBSG_OK;
+  }
   const long slots = split ? sms : (long)sms * gffma_table(pl->ffma_tile).per_sm;
   pl->grid = (int)std::max<long>(1, std::min<long>(slots, L.num_tiles));
   return HBSG_OK;
@@ -959,10 +1059,15 @@ extern "C" {
 size_t hbsg_grouped_workspace_size(int count, const hbsg_problem* problems, int variant,
                                    const hbsg_config* cfg) {
   if (validate(count, problems, variant) != HBSG_OK) return 0;
-  int fi, ti, bm, bn;
-  if (!tile_shape(variant, cfg, &fi, &ti, &bm, &bn)) return 0;
+  int fi, ti, ui, bm, bn;
+  if (!tile_shape(variant, cfg, &fi, &ti, &ui, &bm, &bn)) return 0;
+  const bool fused = ui >= 0;
+  hbsg_config no_inline{};
+  if (cfg) no_inline = *cfg;
+  no_inline.inline_split_pct = -1;
   return grouped_layout(count, problems, variant, bm, bn,
-                        grouped_sets(count, problems, variant, cfg)).total;
+                        grouped_sets(count, problems, variant, fused ? &no_inline : cfg),
+                        fused).total;
 }
 
 int hbsg_grouped_plan_create(hbsg_grouped_plan* out, int count, const hbsg_problem* problems,

@@ -85,18 +85,8 @@ static cudaError_t launch_fused(const FusedParams& p, const TcRun& run, int grid
             : reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, false, false>);
   }
   if (!set_smem_once(k, S::kSmemBytes, &masks[slot])) return cudaErrorInvalidValue;
-  // The body's setmaxnreg split hands out exactly 512 threads x 128
-  // registers; a kernel built with another count would wait forever in
-  // setmaxnreg.inc, so it is never launched.
-  static int regs_ok[4] = {0, 0, 0, 0};  // 0 unchecked, 1 ok, -1 wrong count
-  int st_regs = __atomic_load_n(&regs_ok[slot], __ATOMIC_ACQUIRE);
-  if (st_regs == 0) {
-    cudaFuncAttributes fa;
-    st_regs = (cudaFuncGetAttributes(&fa, k) == cudaSuccess && fa.numRegs == 65536 / kFusedThreads)
-                  ? 1 : -1;
-    __atomic_store_n(&regs_ok[slot], st_regs, __ATOMIC_RELEASE);
-  }
-  if (st_regs != 1) return cudaErrorInvalidConfiguration;
+  static int regs_ok[4] = {0, 0, 0, 0};
+  if (!fused_regs_ok(k, &regs_ok[slot])) return cudaErrorInvalidConfiguration;
   if (scaled) {
     if (vec) tc_fused_kernel<P, BN, STAGES, true, true><<<grid, kFusedThreads, S::kSmemBytes, st>>>(p, run);
     else tc_fused_kernel<P, BN, STAGES, true, false><<<grid, kFusedThreads, S::kSmemBytes, st>>>(p, run);
@@ -115,13 +105,8 @@ struct FusedEntry {
 #define HBSG_FUSED_ENTRY(P, BN, ST) \
   FusedEntry { P, BN, ST, TcFusedShape<P, BN, ST>::kSmemBytes, &launch_fused<P, BN, ST> }
 
-// Ordered as the fused tile ids: 6-product then 3-product, 256 then 64 wide.
-static const FusedEntry kFused[] = {
-    HBSG_FUSED_ENTRY(3, 256, 4),
-    HBSG_FUSED_ENTRY(2, 256, 6),
-    HBSG_FUSED_ENTRY(3, 64, 6),
-    HBSG_FUSED_ENTRY(2, 64, 8),
-};
+#define HBSG_FUSED_ENTRY_COMMA(P, BN, ST) HBSG_FUSED_ENTRY(P, BN, ST),
+static const FusedEntry kFused[] = {HBSG_FUSED_TILE_LIST(HBSG_FUSED_ENTRY_COMMA)};
 static constexpr int kNumFused = sizeof(kFused) / sizeof(kFused[0]);
 
 int fused_num_tiles() { return kNumFused; }
@@ -148,10 +133,7 @@ static int fused_clusters(int idx, bool scaled) {
   if (e.parts == P && e.bn == BN)                                                              \
     k = scaled ? reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, ST, true, true>)        \
                : reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, ST, false, true>);
-  HBSG_FUSED_PICK(3, 256, 4)
-  HBSG_FUSED_PICK(2, 256, 6)
-  HBSG_FUSED_PICK(3, 64, 6)
-  HBSG_FUSED_PICK(2, 64, 8)
+  HBSG_FUSED_TILE_LIST(HBSG_FUSED_PICK)
 #undef HBSG_FUSED_PICK
   if (!k) return 0;
   static uint64_t masks[kNumFused][2];

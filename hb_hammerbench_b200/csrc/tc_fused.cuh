@@ -39,6 +39,15 @@
 
 namespace hbsg {
 
+// Fused tile table (parts, BN, stages), shared by the single-GEMM and grouped
+// launches so that fused tile ids mean the same shape in both: 6-product then
+// 3-product forms, 256 then 64 columns wide.
+#define HBSG_FUSED_TILE_LIST(X) \
+  X(3, 256, 4)                  \
+  X(2, 256, 6)                  \
+  X(3, 64, 6)                   \
+  X(2, 64, 8)
+
 static constexpr int kFusedThreads = 512;
 static constexpr int kConvWarps = 7;
 static constexpr int kConvThreads = kConvWarps * 32;
@@ -106,6 +115,23 @@ HBSG_DEV void st_shared16(uint32_t addr, uint4 v) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y),
                "r"(v.z), "r"(v.w)
                : "memory");
+}
+
+// The body's setmaxnreg split hands out exactly kFusedThreads x 128
+// registers; a kernel built with another register count would wait forever in
+// setmaxnreg.inc, so launchers check the count once (cache: 0 unchecked,
+// 1 ok, -1 wrong) and refuse to launch otherwise.
+static inline bool fused_regs_ok(const void* kernel, int* cache) {
+  int st = __atomic_load_n(cache, __ATOMIC_ACQUIRE);
+  if (st == 0) {
+    cudaFuncAttributes fa;
+    st = (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess &&
+          fa.numRegs * kFusedThreads == 65536)
+             ? 1
+             : -1;
+    __atomic_store_n(cache, st, __ATOMIC_RELEASE);
+  }
+  return st == 1;
 }
 
 HBSG_DEV uint32_t bf162_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t*>(&h); }

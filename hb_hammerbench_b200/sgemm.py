@@ -96,11 +96,26 @@ def sgemm(mat1: torch.Tensor, mat2: torch.Tensor, result: torch.Tensor | None = 
     return result
 
 
+def resolve_config(m: int, n: int, k: int, variant, trans: bool, config):
+    """The schedule a call runs: the caller's config when given, else the
+    autotuner's measured choice for the shape class (row-major operands; the
+    tuner measures those), else None (the library heuristic)."""
+    if config is not None or trans:
+        return config
+    from . import autotune
+    if not autotune.enabled():
+        return None
+    name = variant if isinstance(variant, str) else {v: k_ for k_, v in _lib.VARIANTS.items()}[int(variant)]
+    return autotune.lookup(m, n, k, name.lower())
+
+
 def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, variant="ffma",
          trans_a: bool = False, trans_b: bool = False, config=None,
          workspace: torch.Tensor | None = None) -> torch.Tensor:
     """c = op(a) @ op(b) for 2-D float32 CUDA tensors with unit inner stride.
-    With trans_a, `a` holds A^T (k x m); with trans_b, `b` holds B^T (n x k)."""
+    With trans_a, `a` holds A^T (k x m); with trans_b, `b` holds B^T (n x k).
+    Without a config the autotuner's choice for the shape class is used when
+    one is known (resolve_config)."""
     _check_f32_cuda("a", a)
     _check_f32_cuda("b", b)
     if a.dim() != 2 or b.dim() != 2 or a.stride(1) != 1 or b.stride(1) != 1:
@@ -115,7 +130,7 @@ def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, varian
     if c.dim() != 2 or c.stride(1) != 1 or tuple(c.shape) != (m, n):
         raise ValueError("c must be m x n with unit inner stride")
     v = _variant(variant)
-    cfgp = _config(config)
+    cfgp = _config(resolve_config(m, n, k, variant, trans_a or trans_b, config))
     with torch.cuda.device(a.device):
         need = int(lib().hbsg_gemm_workspace_size_ex(int(trans_a), int(trans_b), m, n, k, v,
                                                      cfgp))
@@ -155,6 +170,13 @@ class GroupedPlan:
         self.As, self.Bs, self.Cs = list(As), list(Bs), list(Cs)
         self.variant = _variant(variant)
         self._arr = _problems(self.As, self.Bs, self.Cs)
+        if config is None and self.As:
+            from . import autotune
+            if autotune.enabled():
+                name = {v: k_ for k_, v in _lib.VARIANTS.items()}[self.variant]
+                dims = [(a.shape[0], b.shape[1], a.shape[1]) for a, b in zip(self.As, self.Bs)]
+                config = autotune.lookup_grouped(dims, name)
+        self.config = config
         self._cfg = _config(config)
         dev = self.As[0].device if self.As else torch.device("cuda")
         with torch.cuda.device(dev):

@@ -52,3 +52,24 @@ def test_tune_grouped(cache):
     for a, b, c in zip(As, Bs, Cs):
         ref = a.double() @ b.double()
         assert (torch.linalg.norm(c.double() - ref) / torch.linalg.norm(ref)).item() < 2e-6
+
+
+def test_tuned_choice_is_the_default(cache, monkeypatch):
+    # with the lookup on, a call without a schedule runs the cached choice for
+    # its shape class: bit-identical to passing that schedule explicitly
+    import torch
+
+    import hb_hammerbench_b200 as hb
+    from hb_hammerbench_b200 import autotune
+    fused = [t["tile"] for t in hb.tiles() if t["fused"] and t["parts"] == 3 and t["bn"] == 256][0]
+    m, n, k = 1000, 900, 1500
+    cfg = {"tile": fused, "split_k": 0, "chunk_k": 32, "raster_group": 8}
+    autotune._store(autotune.shape_key(m, n, k, "bf16x6"), {"config": cfg, "ms": 1.0})
+    monkeypatch.setenv("HBSG_AUTOTUNE", "1")
+    A = torch.rand((m, k), device="cuda") * 2 - 1
+    B = torch.rand((k, n), device="cuda") * 2 - 1
+    assert torch.equal(hb.gemm(A, B, variant="bf16x6"), hb.gemm(A, B, variant="bf16x6", config=cfg))
+    monkeypatch.setenv("HBSG_AUTOTUNE", "0")
+    C0 = hb.gemm(A, B, variant="bf16x6")  # library heuristic: chunk 64, not the cached 32
+    ref = A.double() @ B.double()
+    assert (torch.linalg.norm(C0.double() - ref) / torch.linalg.norm(ref)).item() < 2e-6

@@ -138,3 +138,30 @@ def test_fused_rejects_transposed(hb, fused_ids):
         hb.gemm(A.t().contiguous(), B, variant="bf16x6", trans_a=True,
                 config={"tile": fused[(3, 256)]})
     assert e.value.status == -2
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3", "bf16x6_scaled"])
+@pytest.mark.parametrize("ragged", [False, True])
+def test_grouped_fused_matches_single(hb, fused_ids, variant, ragged):
+    # a grouped plan on the fused tiles computes every problem exactly as the
+    # single-GEMM entry point on the unfused tile of the same width
+    import numpy as np
+    import torch
+    fused, plain = fused_ids
+    P = PARTS[variant]
+    rng = np.random.Generator(np.random.PCG64(17 + ragged))
+    As, Bs = [], []
+    for i in range(20):
+        if ragged:
+            m, n, k = (int(x) for x in rng.integers(1, 700, 3))
+        else:
+            m, n, k = (int(x) for x in rng.integers(2, 21, 3) * 32)
+        As.append(_rand((m, k), 100 + i, "scaled" in variant))
+        Bs.append(_rand((k, n), 200 + i, "scaled" in variant))
+    plan = hb.GroupedPlan(As, Bs, variant=variant, config={"tile": fused[(P, 256)]})
+    Cs = plan.run()
+    torch.cuda.synchronize()
+    for a, b, c in zip(As, Bs, Cs):
+        ref = hb.gemm(a, b, variant=variant, config={"tile": plain[(P, 256)], "split_k": 1})
+        assert torch.equal(c, ref), (tuple(a.shape), tuple(b.shape))
+    plan.close()
