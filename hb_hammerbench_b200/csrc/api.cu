@@ -109,7 +109,7 @@ struct TcChoice {
 // explicitly requested tile does not fit the variant or the operand layout
 // (the fused kernels take row-major operands only).
 static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg, int sms,
-                        bool transposed, TcChoice* ch) {
+                        bool transposed, bool fusable, TcChoice* ch) {
   const int P = parts_of(variant);
   const int tile = cfg && cfg->tile > 0 ? cfg->tile - 1 : -1;
   const int req = cfg ? cfg->split_k : 0;
@@ -119,7 +119,9 @@ static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg
     if (t >= tc_num_tiles()) {
       ch->fused = true;
       ch->idx = t - tc_num_tiles();
-      if (transposed || ch->idx >= fused_num_tiles() || fused_tile_parts(ch->idx) != P) return false;
+      if (transposed || !fusable || ch->idx >= fused_num_tiles() ||
+          fused_tile_parts(ch->idx) != P)
+        return false;
     } else {
       ch->idx = t;
       if (t < 0 || tc_tile_parts(t) != P) return false;
@@ -133,7 +135,7 @@ static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg
 }
 
 static size_t workspace_needed(int M, int N, int K, int batch, int variant, const hbsg_config* cfg,
-                               bool transposed = false) {
+                               bool transposed = false, bool fusable = true) {
   if (variant == HBSG_FFMA) {
     const int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
     return ffma_workspace_bytes(M, N, batch, splits);
@@ -143,7 +145,7 @@ static size_t workspace_needed(int M, int N, int K, int batch, int variant, cons
   const int sms = current_device_sms(nullptr);
   if (sms < 0) return 0;
   TcChoice ch;
-  if (!tc_schedule(M, N, K, variant, cfg, sms, transposed, &ch)) return 0;
+  if (!tc_schedule(M, N, K, variant, cfg, sms, transposed, fusable, &ch)) return 0;
   const size_t partial = ch.splits > 1 ? align256((size_t)ch.splits * M * N * 4) : 0;
   return (ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant)).total + partial;
 }
@@ -202,7 +204,11 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   const int P = parts_of(variant);
   const bool scaled = scaled_of(variant);
   TcChoice ch;
-  if (!tc_schedule(M, N, K, variant, cfg, sms, trans_a || trans_b, &ch))
+  // fused tiles read A and B through FP32 TMA maps (16-byte aligned rows)
+  // (with K = 0 nothing is read)
+  const bool fusable =
+      K == 0 || (fused_operands_ok(A, lda, B, ldb) && strideA % 4 == 0 && strideB % 4 == 0);
+  if (!tc_schedule(M, N, K, variant, cfg, sms, trans_a || trans_b, fusable, &ch))
     return HBSG_ERR_UNSUPPORTED;
   const int tc = ch.idx, splits = ch.splits;
   const SplitLayout L = ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant);

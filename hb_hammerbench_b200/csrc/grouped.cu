@@ -75,7 +75,7 @@ struct GTiles {  // tile source for the tensor-core body (split pass run beforeh
     w.m0 = e.y;
     w.n0 = e.z;
     w.kt0 = 0;
-    w.KT = p.Kp / kBK;
+    w.KT = p.K > 0 ? p.Kp / kBK : 0;  // K = 0: no k-tiles, the epilogue stores zeros
     w.rowmax = p.rowmax;
     w.colmax = p.colmax;
     w.A = p.A;
@@ -95,10 +95,10 @@ __global__ void __launch_bounds__(320, 1) tc_grouped_kernel(const GTiles tiles, 
 // Fused-split form: CTA pairs over 256-row tiles, the split done by the
 // product kernel's converter warps (tc_fused.cuh); no split pass and no parts
 // in the workspace.
-template <int P, int BN, int STAGES, bool SCALED, bool VEC>
+template <int P, int BN, int STAGES, int SSTAGES, bool SCALED>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kFusedThreads, 1)
     tc_grouped_fused_kernel(const GTiles tiles, const TcRun run) {
-  tc_fused_body<P, BN, STAGES, SCALED, VEC>(tiles, run);
+  tc_fused_body<P, BN, STAGES, SSTAGES, SCALED>(tiles, run);
 }
 
 // ---- inline split --------------------------------------------------------------
@@ -593,7 +593,9 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
   L.probs_off = 0;
   L.tiles_off = al(sizeof(GProblem) * (size_t)count, 256);
   L.maps_off = al(L.tiles_off + sizeof(int4) * (size_t)L.num_tiles, 256);
-  L.jobs_off = al(L.maps_off + (parts_in_hbm ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
+  // two tensor maps per problem: its BF16 parts (split pass) or, fused, its
+  // FP32 operands
+  L.jobs_off = al(L.maps_off + (split ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
   const long jobs = L.num_jobs_a + L.num_jobs_b + L.num_jobs_rmax + L.num_jobs_cmax;
   L.sync_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);
   L.sync_bytes = inline_split ? al(sizeof(int) * ((size_t)count + 1), 256) : 0;
@@ -700,39 +702,16 @@ static uint64_t g_tc_masks[sizeof(kGTc) / sizeof(kGTc[0])][2];
 
 struct GFusedEntry {
   int smem;
-  const void* k[4];  // [scaled * 2 + vec]
+  const void* k[2];  // [scaled]
 };
-#define HBSG_GFUSED_ENTRY(P, BN, ST)                                                       \
-  GFusedEntry{TcFusedShape<P, BN, ST>::kSmemBytes,                                         \
-              {reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, false, false>), \
-               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, false, true>),  \
-               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, true, false>),  \
-               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, true, true>)}},
+#define HBSG_GFUSED_ENTRY(P, BN, ST, SST)                                                     \
+  GFusedEntry{TcFusedShape<P, BN, ST, SST>::kSmemBytes,                                       \
+              {reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, SST, false>), \
+               reinterpret_cast<const void*>(&tc_grouped_fused_kernel<P, BN, ST, SST, true>)}},
 static const GFusedEntry kGFused[] = {HBSG_FUSED_TILE_LIST(HBSG_GFUSED_ENTRY)};
 static constexpr int kNumGFused = sizeof(kGFused) / sizeof(kGFused[0]);
-static uint64_t g_fused_masks[kNumGFused][4];
-static int g_fused_regs[kNumGFused][4];
-
-// Co-resident clusters of two CTAs of a grouped fused kernel (0 if unknown).
-static int gfused_clusters(const void* k, int smem) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(2, 1, 1);
-  cfg.blockDim = dim3(kFusedThreads, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cudaLaunchAttribute attr;
-  attr.id = cudaLaunchAttributeClusterDimension;
-  attr.val.clusterDim.x = 2;
-  attr.val.clusterDim.y = 1;
-  attr.val.clusterDim.z = 1;
-  cfg.attrs = &attr;
-  cfg.numAttrs = 1;
-  int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  return n;
-}
+static uint64_t g_fused_masks[kNumGFused][2];
+static int g_fused_regs[kNumGFused][2];
 
 // Launches of one grouped product on `st` (no host synchronisation, no
 // allocation: capturable).
@@ -792,7 +771,7 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
   gt.n = (int)L.num_tiles;
   TcRun run = pl.run;
   if (pl.fused_tile >= 0) {
-    const int slot = (scaled ? 2 : 0) + (pl.vec ? 1 : 0);
+    const int slot = scaled ? 1 : 0;
     const GFusedEntry& fe = kGFused[pl.fused_tile];
     const void* k = fe.k[slot];
     if (!set_smem_once(k, fe.smem, &g_fused_masks[pl.fused_tile][slot]))
@@ -964,18 +943,18 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
           for (int k0 = 0; k0 < g.K; k0 += 256) jobs.push_back(make_int4(i, n0, k0, 0));
       }
     }
-    if (!fused) {
-      maps.resize(2 * (size_t)count);
-      for (int i = 0; i < count; ++i) {
-        const GProblem& g = probs[i];
-        if (g.M <= 0 || g.N <= 0) {
-          memset(&maps[2 * i], 0, 2 * sizeof(CUtensorMap));
-          continue;
-        }
-        if (!tc_make_parts_map(&maps[2 * i], g.Ap, P, g.M, g.Kp, kBM) ||
-            !tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp, bn))
-          return HBSG_ERR_UNSUPPORTED;
+    maps.resize(2 * (size_t)count);
+    for (int i = 0; i < count; ++i) {
+      const GProblem& g = probs[i];
+      if (g.M <= 0 || g.N <= 0 || (fused && g.K <= 0)) {  // nothing is loaded for these
+        memset(&maps[2 * i], 0, 2 * sizeof(CUtensorMap));
+        continue;
       }
+      const bool ok = fused ? fused_make_maps(pl->fused_tile, g.A, g.lda, g.B, g.ldb, g.M, g.N,
+                                              g.K, &maps[2 * i], &maps[2 * i + 1])
+                            : tc_make_parts_map(&maps[2 * i], g.Ap, P, g.M, g.Kp, kBM) &&
+                                  tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp, bn);
+      if (!ok) return HBSG_ERR_UNSUPPORTED;
     }
     pl->run.chunk_ktiles = tc_chunk_ktiles(P, cfg ? cfg->chunk_k : 0);
     pl->run.l2_ahead = tc_l2_ahead();
@@ -1022,11 +1001,11 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
 
   if (fused) {
     // CTA pairs: grid = 2 x min(tiles, co-resident clusters)
-    const int slot = (scaled ? 2 : 0) + (pl->vec ? 1 : 0);
+    const int slot = scaled ? 1 : 0;
     const GFusedEntry& fe = kGFused[pl->fused_tile];
     if (!set_smem_once(fe.k[slot], fe.smem, &g_fused_masks[pl->fused_tile][slot]))
       return HBSG_ERR_LAUNCH;
-    int resident = gfused_clusters(fe.k[slot], fe.smem);
+    int resident = fused_resident_clusters(fe.k[slot], fe.smem);
     if (resident <= 0 || resident > sms / 2) resident = sms / 2;
     pl->grid = (int)(2 * std::max<long>(1, std::min<long>(resident, L.num_tiles)));
     return HBSG_OK;

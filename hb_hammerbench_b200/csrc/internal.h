@@ -83,6 +83,16 @@ int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int*
 cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sms,
                          unsigned long long wait_limit_ns, cudaStream_t st, float* partial);
 int fused_read_and_clear_device_error();
+// Fused kernels read A and B through FP32 TMA maps: 16-byte aligned bases and
+// row strides that are multiples of 4 floats.
+bool fused_operands_ok(const float* A, long lda, const float* B, long ldb);
+// The two FP32 tensor maps (CUtensorMap, 128 bytes each) of fused entry idx.
+bool fused_make_maps(int idx, const float* A, long lda, const float* B, long ldb, int M, int N,
+                     int K, void* map_a, void* map_b);
+// 2-D FP32 map over rows of `inner` elements (row stride ld elements), box
+// {box_inner, box_outer}, 128-byte swizzle or none; zeros outside the matrix.
+bool tc_make_f32_map(void* map, const void* base, int inner, int outer, long ld, int box_inner,
+                     int box_outer, bool swizzle128);
 // K slices of the automatic schedule for `tiles` output tiles on `slots`
 // concurrent work slots (requested > 0 overrides); shared by both families.
 int tc_slices(long tiles, int K, int slots, int requested, int* kt_per_split);

@@ -7,8 +7,11 @@
 // the unfused kernel (tc_gemm.cu): with K slices each slice writes an FP32
 // partial to the workspace, reduced in fixed order afterwards. The scaled
 // forms read per-row / per-column maxima that a max pass computes first
-// (split_bf16.cu); nothing else is staged in HBM.
+// (split_bf16.cu); nothing else is staged in HBM. The kernel reads A and B
+// through two FP32 TMA tensor maps, so both need 16-byte aligned bases and
+// row strides (lda, ldb multiples of 4 floats).
 #include <algorithm>
+#include <cstring>
 
 #include "tc_fused.cuh"
 
@@ -17,6 +20,8 @@ namespace hbsg {
 struct FusedTiles {
   static constexpr bool kInlineSplit = false;
   const FusedParams* p;
+  const CUtensorMap* ma;  // FP32 A, box {32, 128}
+  const CUtensorMap* mb;  // FP32 B, box {BN/2, 32}
   __device__ __forceinline__ int count() const { return p->num_tiles * p->splits; }
   template <int BN>
   __device__ __forceinline__ TileWork get_bn(int item) const {
@@ -30,8 +35,8 @@ struct FusedTiles {
     TileWork w;
     w.prob = 0;
     w.ready_target = 0;
-    w.ma = nullptr;
-    w.mb = nullptr;
+    w.ma = ma;
+    w.mb = mb;
     w.M = p->M;
     w.N = p->N;
     w.m0 = (first + in % gm) * (2 * kBM);
@@ -62,51 +67,59 @@ struct FusedTilesBN : FusedTiles {
   __device__ __forceinline__ TileWork get(int t) const { return get_bn<BN>(t); }
 };
 
-template <int P, int BN, int STAGES, bool SCALED, bool VEC>
+template <int P, int BN, int STAGES, int SSTAGES, bool SCALED>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kFusedThreads, 1)
-    tc_fused_kernel(const __grid_constant__ FusedParams p, const TcRun run) {
+    tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    const __grid_constant__ FusedParams p, const TcRun run) {
   FusedTilesBN<BN> tiles;
   tiles.p = &p;
-  tc_fused_body<P, BN, STAGES, SCALED, VEC>(tiles, run);
+  tiles.ma = &tmA;
+  tiles.mb = &tmB;
+  tc_fused_body<P, BN, STAGES, SSTAGES, SCALED>(tiles, run);
 }
 
-template <int P, int BN, int STAGES>
-static cudaError_t launch_fused(const FusedParams& p, const TcRun& run, int grid, cudaStream_t st,
-                                bool scaled, bool vec) {
-  using S = TcFusedShape<P, BN, STAGES>;
-  const void* k;
-  static uint64_t masks[4] = {0, 0, 0, 0};
-  const int slot = (scaled ? 2 : 0) + (vec ? 1 : 0);
-  if (scaled) {
-    k = vec ? reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, true, true>)
-            : reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, true, false>);
-  } else {
-    k = vec ? reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, false, true>)
-            : reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, false, false>);
-  }
-  if (!set_smem_once(k, S::kSmemBytes, &masks[slot])) return cudaErrorInvalidValue;
-  static int regs_ok[4] = {0, 0, 0, 0};
-  if (!fused_regs_ok(k, &regs_ok[slot])) return cudaErrorInvalidConfiguration;
-  if (scaled) {
-    if (vec) tc_fused_kernel<P, BN, STAGES, true, true><<<grid, kFusedThreads, S::kSmemBytes, st>>>(p, run);
-    else tc_fused_kernel<P, BN, STAGES, true, false><<<grid, kFusedThreads, S::kSmemBytes, st>>>(p, run);
-  } else {
-    if (vec) tc_fused_kernel<P, BN, STAGES, false, true><<<grid, kFusedThreads, S::kSmemBytes, st>>>(p, run);
-    else tc_fused_kernel<P, BN, STAGES, false, false><<<grid, kFusedThreads, S::kSmemBytes, st>>>(p, run);
-  }
+template <int P, int BN, int STAGES, int SSTAGES>
+static const void* fused_kernel_ptr(bool scaled) {
+  return scaled ? reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, SSTAGES, true>)
+                : reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, STAGES, SSTAGES, false>);
+}
+
+template <int P, int BN, int STAGES, int SSTAGES>
+static cudaError_t launch_fused(const CUtensorMap& a, const CUtensorMap& b, const FusedParams& p,
+                                const TcRun& run, int grid, cudaStream_t st, bool scaled) {
+  using S = TcFusedShape<P, BN, STAGES, SSTAGES>;
+  const void* k = fused_kernel_ptr<P, BN, STAGES, SSTAGES>(scaled);
+  static uint64_t masks[2] = {0, 0};
+  if (!set_smem_once(k, S::kSmemBytes, &masks[scaled ? 1 : 0])) return cudaErrorInvalidValue;
+  static int regs_ok[2] = {0, 0};
+  if (!fused_regs_ok(k, &regs_ok[scaled ? 1 : 0])) return cudaErrorInvalidConfiguration;
+  if (scaled)
+    tc_fused_kernel<P, BN, STAGES, SSTAGES, true><<<grid, kFusedThreads, S::kSmemBytes, st>>>(a, b, p, run);
+  else
+    tc_fused_kernel<P, BN, STAGES, SSTAGES, false><<<grid, kFusedThreads, S::kSmemBytes, st>>>(a, b, p, run);
   return cudaGetLastError();
 }
 
+template <int P, int BN, int STAGES, int SSTAGES>
+static int fused_clusters_of(bool scaled) {
+  using S = TcFusedShape<P, BN, STAGES, SSTAGES>;
+  const void* k = fused_kernel_ptr<P, BN, STAGES, SSTAGES>(scaled);
+  static uint64_t masks[2] = {0, 0};
+  if (!set_smem_once(k, S::kSmemBytes, &masks[scaled ? 1 : 0])) return 0;
+  return fused_resident_clusters(k, S::kSmemBytes);
+}
+
 struct FusedEntry {
-  int parts, bn, stages, smem;
-  cudaError_t (*launch)(const FusedParams&, const TcRun&, int, cudaStream_t, bool, bool);
+  int parts, bn, stages, sstages, smem;
+  cudaError_t (*launch)(const CUtensorMap&, const CUtensorMap&, const FusedParams&, const TcRun&,
+                        int, cudaStream_t, bool);
+  int (*clusters)(bool);
 };
 
-#define HBSG_FUSED_ENTRY(P, BN, ST) \
-  FusedEntry { P, BN, ST, TcFusedShape<P, BN, ST>::kSmemBytes, &launch_fused<P, BN, ST> }
-
-#define HBSG_FUSED_ENTRY_COMMA(P, BN, ST) HBSG_FUSED_ENTRY(P, BN, ST),
-static const FusedEntry kFused[] = {HBSG_FUSED_TILE_LIST(HBSG_FUSED_ENTRY_COMMA)};
+#define HBSG_FUSED_ENTRY(P, BN, ST, SST)                                                   \
+  FusedEntry{P, BN, ST, SST, TcFusedShape<P, BN, ST, SST>::kSmemBytes,                    \
+             &launch_fused<P, BN, ST, SST>, &fused_clusters_of<P, BN, ST, SST>},
+static const FusedEntry kFused[] = {HBSG_FUSED_TILE_LIST(HBSG_FUSED_ENTRY)};
 static constexpr int kNumFused = sizeof(kFused) / sizeof(kFused[0]);
 
 int fused_num_tiles() { return kNumFused; }
@@ -125,46 +138,34 @@ bool fused_tile_info(int idx, hbsg_tile_info* out) {
   return true;
 }
 
-// Co-resident clusters of two CTAs of fused entry `idx` (0 if unknown).
-static int fused_clusters(int idx, bool scaled) {
-  const FusedEntry& e = kFused[idx];
-  const void* k = nullptr;
-#define HBSG_FUSED_PICK(P, BN, ST)                                                             \
-  if (e.parts == P && e.bn == BN)                                                              \
-    k = scaled ? reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, ST, true, true>)        \
-               : reinterpret_cast<const void*>(&tc_fused_kernel<P, BN, ST, false, true>);
-  HBSG_FUSED_TILE_LIST(HBSG_FUSED_PICK)
-#undef HBSG_FUSED_PICK
-  if (!k) return 0;
-  static uint64_t masks[kNumFused][2];
-  if (!set_smem_once(k, e.smem, &masks[idx][scaled ? 1 : 0])) return 0;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(2, 1, 1);
-  cfg.blockDim = dim3(kFusedThreads, 1, 1);
-  cfg.dynamicSmemBytes = e.smem;
-  cudaLaunchAttribute attr;
-  attr.id = cudaLaunchAttributeClusterDimension;
-  attr.val.clusterDim.x = 2;
-  attr.val.clusterDim.y = 1;
-  attr.val.clusterDim.z = 1;
-  cfg.attrs = &attr;
-  cfg.numAttrs = 1;
-  int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  return n;
-}
-
 int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
   const long tiles = (long)((M + 2 * kBM - 1) / (2 * kBM)) * ((N + kFused[idx].bn - 1) / kFused[idx].bn);
   return tc_slices(tiles, K, sms / 2, requested, kt_per_split);
 }
 
+bool fused_operands_ok(const float* A, long lda, const float* B, long ldb) {
+  return ((lda & 3) == 0) && ((ldb & 3) == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
+         ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
+}
+
+bool fused_make_maps(int idx, const float* A, long lda, const float* B, long ldb, int M, int N,
+                     int K, void* map_a, void* map_b) {
+  if (!fused_operands_ok(A, lda, B, ldb)) return false;
+  return tc_make_f32_map(map_a, A, K, M, lda, kBK, kBM, true) &&
+         tc_make_f32_map(map_b, B, N, K, ldb, kFused[idx].bn / 2, kBK, false);
+}
+
 cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sms,
                          unsigned long long wait_limit_ns, cudaStream_t st, float* partial) {
   const FusedEntry& e = kFused[idx];
+  CUtensorMap ma, mb;
+  if (p.K > 0) {
+    if (!fused_make_maps(idx, p.A, p.lda, p.B, p.ldb, p.M, p.N, p.K, &ma, &mb))
+      return cudaErrorInvalidValue;
+  } else {  // no k-tiles: nothing is loaded, the epilogue stores zeros
+    memset(&ma, 0, sizeof(ma));
+    memset(&mb, 0, sizeof(mb));
+  }
   p.tiles_m = (p.M + 2 * kBM - 1) / (2 * kBM);
   p.tiles_n = (p.N + e.bn - 1) / e.bn;
   p.num_tiles = p.tiles_m * p.tiles_n;
@@ -182,14 +183,13 @@ cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sm
   run.debug_skip_loads = 0;
   run.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;
   const bool scaled = p.rowmax != nullptr;
-  const bool vec = ((p.lda & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.A) & 15) == 0);
   const long items = (long)p.num_tiles * p.splits;
   // pairs never wait on each other, so a grid larger than what is resident
   // would only run late; it is capped at the co-resident clusters
-  int resident = fused_clusters(idx, scaled);
-  if (resident <= 0) resident = sms / 2;
-  const long pairs = std::max<long>(1, std::min<long>(items, std::min(resident, sms / 2)));
-  cudaError_t err = e.launch(p, run, (int)(2 * pairs), st, scaled, vec);
+  int resident = e.clusters(scaled);
+  if (resident <= 0 || resident > sms / 2) resident = sms / 2;
+  const long pairs = std::max<long>(1, std::min<long>(items, resident));
+  cudaError_t err = e.launch(ma, mb, p, run, (int)(2 * pairs), st, scaled);
   if (err != cudaSuccess || p.splits == 1) return err;
   return splitk_reduce(partial, C, p.M, p.N, ldc, 0, p.splits, 1, sms, st);
 }

@@ -5,33 +5,38 @@
 // pass and the product kernel reads them back: for an operand element that is
 // 4 bytes read + 2*P written + 2*P read again, against the 4 bytes the
 // product needs. Here the product kernel reads the FP32 operands itself:
-// converter warps load FP32 A rows and B columns with coalesced global loads
-// one k-tile ahead, split every value into P parts (exactly the split pass's
-// arithmetic: hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid)) and
-// write them into the shared-memory stage in the layout the TMA produced
-// before (K-major rows of 32 bf16 = 64 bytes, 64-byte swizzle: the 16-byte
-// chunk c of row r lands at chunk c ^ ((r >> 1) & 3)). The MMA issuer and the
-// epilogue are those of the pair kernel (tc_kernel2.cuh): same products, same
-// order, same TMEM drains, so the result is bit-identical to the unfused
-// kernels with the same drain interval.
+//   - a loader thread streams this CTA's FP32 A rows and B columns of each
+//     k-tile into a shared-memory staging ring with TMA (no registers held in
+//     flight, so the ring can run several k-tiles ahead of DRAM latency);
+//   - converter warps read a staged k-tile, split every value into P parts
+//     (exactly the split pass's arithmetic: hi = bf16(x), mid = bf16(x - hi),
+//     lo = bf16(x - hi - mid)) and write them into the operand stage in the
+//     layout the TMA produced for the unfused kernel (K-major rows of 32 bf16
+//     = 64 bytes, 64-byte swizzle: the 16-byte chunk c of row r lands at chunk
+//     c ^ ((r >> 1) & 3));
+//   - the MMA issuer and the epilogue are those of the pair kernel
+//     (tc_kernel2.cuh): same products, same order, same TMEM drains, so the
+//     result is bit-identical to the unfused kernels with the same drain
+//     interval.
 //
 // Why CTA pairs: the tensor core's shared-memory operand reads per MMA flop
 // are lowest for the 256 x 256 pair tile (each SM holds 128 A rows and 128 B
-// columns: ~64 of the 128 bytes/clock an SM's shared memory moves). The
-// converters' part writes add ~32 bytes/clock (6-product form), which still
-// fits; on a single-CTA 128 x 256 tile the MMA alone reads ~96 bytes/clock
-// and the writes would not fit.
+// columns). Staging and converting add shared-memory traffic (FP32 written by
+// the TMA, read by the converters, parts written), which a single-CTA
+// 128 x 256 tile, whose MMA alone reads ~3/4 of an SM's shared-memory
+// bandwidth, has no room for.
 //
 // CTA (512 threads, 16 warps, one CTA per SM, clusters of two):
 //   warp 0       TMEM allocation; lane 0 of the leader CTA issues the MMAs
-//   warps 1-7    converters (this CTA's 128 A rows and BN/2 B columns)
+//   warp 1       lane 0: TMA loads of the FP32 staging ring
+//   warps 2-7    converters (this CTA's 128 A rows and BN/2 B columns)
 //   warps 8-15   epilogue (TMEM lane quadrant warp % 4, column half)
-// Register split (setmaxnreg): warpgroups 0-1 (issuer, converters) 104
-// registers per thread, warpgroups 2-3 (epilogue, BN/2 FP32 sums per thread)
-// 152: 2 x 128 x 104 + 2 x 128 x 152 = 65536, the block's launch allotment
-// (512 threads x 128). ptxas reports no spills for any instantiation at this
-// split (it spilled at 80/176, 88/168 and 96/160).
-// Every wait is bounded as in the other tensor-core bodies; no TMA is used.
+// Register split (setmaxnreg): warpgroups 0-1 (issuer, loader, converters,
+// which hold one 8-value unit at a time) 72 registers per thread, warpgroups
+// 2-3 (epilogue, BN/2 FP32 sums per thread) 184: 2 x 128 x 72 + 2 x 128 x 184
+// = 65536, the block's launch allotment (512 threads x 128).
+// Every wait is bounded as in the other tensor-core bodies. The TMA loads use
+// no cluster multicast: each CTA loads its own rows into its own memory.
 #pragma once
 
 #include "split_kernel.cuh"
@@ -39,20 +44,20 @@
 
 namespace hbsg {
 
-// Fused tile table (parts, BN, stages), shared by the single-GEMM and grouped
-// launches so that fused tile ids mean the same shape in both: 6-product then
-// 3-product forms, 256 then 64 columns wide.
+// Fused tile table (parts, BN, part stages, FP32 staging stages), shared by
+// the single-GEMM and grouped launches so that fused tile ids mean the same
+// shape in both: 6-product then 3-product forms, 256 then 64 columns wide.
 #define HBSG_FUSED_TILE_LIST(X) \
-  X(3, 256, 4)                  \
-  X(2, 256, 6)                  \
-  X(3, 64, 6)                   \
-  X(2, 64, 8)
+  X(3, 256, 2, 3)               \
+  X(2, 256, 3, 3)               \
+  X(3, 64, 3, 4)                \
+  X(2, 64, 4, 4)
 
 static constexpr int kFusedThreads = 512;
-static constexpr int kConvWarps = 7;
+static constexpr int kConvWarps = 6;
 static constexpr int kConvThreads = kConvWarps * 32;
-static constexpr int kRegsLow = 104;   // warpgroups 0-1
-static constexpr int kRegsHigh = 152;  // warpgroups 2-3
+static constexpr int kRegsLow = 72;    // warpgroups 0-1
+static constexpr int kRegsHigh = 184;  // warpgroups 2-3
 static_assert(2 * 128 * kRegsLow + 2 * 128 * kRegsHigh == 65536, "register split");
 
 // mbarrier probe with cluster-scope acquire: the converters of the peer CTA
@@ -98,19 +103,6 @@ HBSG_DEV void regs_inc() {
   asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(N));
 }
 
-HBSG_DEV float ldg_stream(const float* p) {
-  float v;
-  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-}
-HBSG_DEV float4 ldg_stream4(const float* p) {
-  float4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "l"(p));
-  return v;
-}
-
 HBSG_DEV void st_shared16(uint32_t addr, uint4 v) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y),
                "r"(v.z), "r"(v.w)
@@ -132,6 +124,27 @@ static inline bool fused_regs_ok(const void* kernel, int* cache) {
     __atomic_store_n(cache, st, __ATOMIC_RELEASE);
   }
   return st == 1;
+}
+
+// Co-resident clusters of two CTAs of a fused kernel (0 if unknown).
+static inline int fused_resident_clusters(const void* kernel, int smem) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kFusedThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = 2;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
 }
 
 HBSG_DEV uint32_t bf162_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t*>(&h); }
@@ -182,16 +195,21 @@ HBSG_DEV void split8(float (&x)[8], int e, uint4 (&out)[P]) {
   if constexpr (P == 3) out[2] = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-template <int P, int BN, int STAGES>
+template <int P, int BN, int STAGES, int SSTAGES>
 struct TcFusedShape {
   static constexpr int kHalf = BN / 2;                  // B columns per CTA
   static constexpr int kABytes = kBM * kBK * 2;         // 128 rows of one part
   static constexpr int kBBytes = kHalf * kBK * 2;       // this CTA's B columns, one part
   static constexpr int kStageBytes = P * (kABytes + kBBytes);
+  static constexpr int kSABytes = kBM * kBK * 4;        // FP32 A staging: 128 rows x 32 k
+  static constexpr int kSBBytes = kBK * kHalf * 4;      // FP32 B staging: 32 k x BN/2 columns
+  static constexpr int kSStageBytes = kSABytes + kSBBytes;
   static constexpr int kAllocCols = 2 * BN <= 32 ? 32 : 2 * BN <= 64 ? 64 : 2 * BN <= 128 ? 128 : 2 * BN <= 256 ? 256 : 512;
-  static constexpr int kBarBytes = 8 * (2 * STAGES + 4) + 16;
+  static constexpr int kBarBytes = 8 * (2 * STAGES + 4 + 2 * SSTAGES) + 16;
   static constexpr int kColExpBytes = 8 * 4 * (BN / 2);
-  static constexpr int kSmemBytes = 1024 + STAGES * kStageBytes + kBarBytes + kColExpBytes;
+  static constexpr int kStagingOff = STAGES * kStageBytes;
+  static constexpr int kBarOff = kStagingOff + SSTAGES * kSStageBytes;
+  static constexpr int kSmemBytes = 1024 + kBarOff + kBarBytes + kColExpBytes;
   // converter work per k-tile: 8-element units (one row of A or column of B,
   // 8 consecutive k); A units first: unit u < kAUnits is row u / 4, chunk u % 4
   static constexpr int kAUnits = kBM * 4;
@@ -201,6 +219,8 @@ struct TcFusedShape {
   static_assert(kSmemBytes <= 232448, "shared memory");
   static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256, "pair UMMA N");
   static_assert(kBBytes % 512 == 0, "B part base keeps the 512-byte swizzle alignment");
+  static_assert(kStageBytes % 1024 == 0 && kSStageBytes % 1024 == 0 && kSABytes % 1024 == 0,
+                "FP32 A staging keeps the 1024-byte alignment of the 128-byte swizzle");
   static_assert(kAUnits % 32 == 0, "a warp's units are all A or all B");
 };
 
@@ -210,21 +230,38 @@ HBSG_DEV uint32_t sw64_offset(int r, int c) {
   return (uint32_t)(r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
 }
 
-template <int P, int BN, int STAGES, bool SCALED, bool VEC, class Tiles>
+// Byte offset of the 16-byte chunk c (4 floats) of row r in the FP32 A
+// staging tile (128-byte rows, 128-byte swizzle: address bits 4-6 ^= bits 7-9).
+HBSG_DEV uint32_t sw128_offset(int r, int c) {
+  return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
+}
+
+HBSG_DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int P, int BN, int STAGES, int SSTAGES, bool SCALED, class Tiles>
 __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& run) {
-  using S = TcFusedShape<P, BN, STAGES>;
+  using S = TcFusedShape<P, BN, STAGES, SSTAGES>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* smem = smem_raw + (base - raw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * S::kStageBytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::kBarOff);
   uint64_t* full = bars;                     // leader: both CTAs' converters filled the stage
   uint64_t* empty = bars + STAGES;           // each CTA: the stage is free again
   uint64_t* tfull = bars + 2 * STAGES;       // each CTA: accumulator buffer ready
   uint64_t* tempty = bars + 2 * STAGES + 2;  // leader: both CTAs drained the buffer
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
+  uint64_t* sfull = bars + 2 * STAGES + 4;   // each CTA: FP32 staging loaded (TMA)
+  uint64_t* sempty = sfull + SSTAGES;        // each CTA: FP32 staging read by the converters
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sempty + SSTAGES);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  int* col_exp = reinterpret_cast<int*>(smem + STAGES * S::kStageBytes + S::kBarBytes);
+  int* col_exp = reinterpret_cast<int*>(smem + S::kBarOff + S::kBarBytes);
+  const uint32_t staging = base + S::kStagingOff;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -243,6 +280,10 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 16);
     }
+    for (int s = 0; s < SSTAGES; ++s) {
+      mbar_init(&sfull[s], 1);
+      mbar_init(&sempty[s], kConvWarps);
+    }
     *abort_flag = 0;
     fence_barrier_init();
   }
@@ -258,12 +299,9 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
   const uint32_t tmem_base = *tmem_slot;
   const unsigned long long lim = run.wait_limit_ns;
 
-  if (warp < 8) {
-    regs_dec<kRegsLow>();
-  } else {
-    regs_inc<kRegsHigh>();
-  }
-
+  // Each role's code sits inside the branch that set its register count, so
+  // the compiler allocates the epilogue's sums under the larger limit.
+  if (warp < 8) regs_dec<kRegsLow>();
   if (warp == 0) {
     // ---------------- MMA issuer (leader CTA only) ----------------
     if (leader && lane == 0) {
@@ -312,106 +350,126 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
         }
       }
     }
+  } else if (warp == 1) {
+    // ---------------- TMA loader of the FP32 staging ring (both CTAs) ----------------
+    // This CTA's 128 A rows x 32 k (box {32, 128}, 128-byte swizzle) and its
+    // 32 k x BN/2 B columns (box {BN/2, 32}); rows and columns beyond the
+    // matrix and k beyond K arrive as zeros (out-of-bounds fill).
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      const CUtensorMap* last = nullptr;
+      for (int t = pair; t < num_tiles && ok; t += pairs) {
+        const TileWork w = tiles.get(t);
+        if (w.ma != last) {
+          asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(w.ma)) : "memory");
+          asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(w.mb)) : "memory");
+          last = w.ma;
+        }
+        const int arow = w.m0 + kBM * (int)rank;
+        const int bcol = w.n0 + S::kHalf * (int)rank;
+        for (int kt = 0; kt < w.KT; ++kt, ++it) {
+          const int ss = it % SSTAGES;
+          if (!wait_bounded(&sempty[ss], ((it / SSTAGES) & 1) ^ 1, abort_flag, lim)) {
+            ok = false;
+            break;
+          }
+          const uint32_t dst = staging + ss * S::kSStageBytes;
+          const int k0 = (w.kt0 + kt) * kBK;
+          mbar_arrive_expect_tx(&sfull[ss], S::kSStageBytes);
+          tma_load_2d(dst, w.ma, k0, arow, &sfull[ss]);
+          tma_load_2d(dst + S::kSABytes, w.mb, bcol, k0, &sfull[ss]);
+        }
+      }
+    }
   } else if (warp < 8) {
     // ---------------- converters (both CTAs) ----------------
     constexpr int NU = S::kUnitsPerThread;
-    const int cid = threadIdx.x - 32;
+    const int cid = threadIdx.x - 64;
     const uint32_t full_leader0 = map_to_rank(smem_u32(&full[0]), 0);
-    float v[NU][8];
     int ex[NU];
 #pragma unroll
     for (int i = 0; i < NU; ++i) ex[i] = 0;
-
-    // Loads unit i of k-tile kt of work item w into v[i] (zeros outside the
-    // matrix and beyond K), and its row/column exponent (scaled forms).
-    auto load_units = [&](const TileWork& w, int kt) {
-      const int kb = (w.kt0 + kt) * kBK;
+    uint32_t it = 0;
+    bool ok = true;
+    for (int t = pair; t < num_tiles && ok; t += pairs) {
+      const TileWork w = tiles.get(t);
+      if constexpr (SCALED) {
+        // the split exponent of each unit's row or column, fixed for the tile
 #pragma unroll
-      for (int i = 0; i < NU; ++i) {
-        const int u = cid + i * kConvThreads;
-        if (u >= S::kUnits) continue;
-        if (u < S::kAUnits) {
-          const int m = w.m0 + kBM * (int)rank + (u >> 2);
-          const int k = kb + (u & 3) * 8;
-          if (m < w.M) {
-            const float* src = w.A + (long)m * w.lda + k;
-            if (VEC && k + 8 <= w.K) {
-              const float4 a0 = ldg_stream4(src);
-              const float4 a1 = ldg_stream4(src + 4);
-              v[i][0] = a0.x; v[i][1] = a0.y; v[i][2] = a0.z; v[i][3] = a0.w;
-              v[i][4] = a1.x; v[i][5] = a1.y; v[i][6] = a1.z; v[i][7] = a1.w;
-            } else {
-#pragma unroll
-              for (int j = 0; j < 8; ++j) v[i][j] = k + j < w.K ? ldg_stream(src + j) : 0.0f;
-            }
-            if constexpr (SCALED) ex[i] = exp_from_maxbits(w.rowmax[m]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) v[i][j] = 0.0f;
-          }
-        } else {
-          const int ub = u - S::kAUnits;
-          const int n = w.n0 + S::kHalf * (int)rank + ub % S::kHalf;
-          const int k = kb + (ub / S::kHalf) * 8;
-          if (n < w.N) {
-            const float* src = w.B + (long)k * w.ldb + n;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) v[i][j] = k + j < w.K ? ldg_stream(src + (long)j * w.ldb) : 0.0f;
-            if constexpr (SCALED) ex[i] = exp_from_maxbits(w.colmax[n]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) v[i][j] = 0.0f;
+        for (int i = 0; i < NU; ++i) {
+          const int u = cid + i * kConvThreads;
+          ex[i] = 0;
+          if (u < S::kAUnits) {
+            const int m = w.m0 + kBM * (int)rank + (u >> 2);
+            if (m < w.M) ex[i] = exp_from_maxbits(w.rowmax[m]);
+          } else if (u < S::kUnits) {
+            const int n = w.n0 + S::kHalf * (int)rank + (u - S::kAUnits) % S::kHalf;
+            if (n < w.N) ex[i] = exp_from_maxbits(w.colmax[n]);
           }
         }
       }
-    };
-
-    uint32_t it = 0;
-    bool ok = true;
-    if (pair < num_tiles) load_units(tiles.get(pair), 0);
-    for (int t = pair; t < num_tiles && ok; t += pairs) {
-      // the work item is re-derived here rather than carried over from the
-      // previous item's prefetch, so only one item's fields stay live
-      const TileWork w = tiles.get(t);
       for (int kt = 0; kt < w.KT; ++kt, ++it) {
         const int s = it % STAGES;
-        if (!wait_bounded(&empty[s], ((it / STAGES) & 1) ^ 1, abort_flag, lim)) {
+        const int ss = it % SSTAGES;
+        if (!wait_bounded(&sfull[ss], (it / SSTAGES) & 1, abort_flag, lim) ||
+            !wait_bounded(&empty[s], ((it / STAGES) & 1) ^ 1, abort_flag, lim)) {
           ok = false;
           break;
         }
         const uint32_t sa = base + s * S::kStageBytes;
         const uint32_t sb = sa + P * S::kABytes;
+        const uint32_t fa = staging + ss * S::kSStageBytes;
+        const uint32_t fb = fa + S::kSABytes;
+        // plain (non-volatile) shared-memory accesses: the compiler may
+        // overlap one unit's loads with the previous unit's arithmetic; the
+        // barrier waits above and the proxy fence below order them against
+        // the TMA writes and the tensor-core reads
+        const uint8_t* fa_p = smem + (fa - base);
+        const uint8_t* fb_p = smem + (fb - base);
+        uint8_t* sa_p = smem + (sa - base);
+        uint8_t* sb_p = smem + (sb - base);
 #pragma unroll
         for (int i = 0; i < NU; ++i) {
           const int u = cid + i * kConvThreads;
           if (u >= S::kUnits) continue;
-          uint4 o[P];
-          split8<P, SCALED>(v[i], ex[i], o);
+          float v[8];
           if (u < S::kAUnits) {
-            const uint32_t off = sw64_offset(u >> 2, u & 3);
+            const int r = u >> 2, c = u & 3;
+            const float4 a0 = *reinterpret_cast<const float4*>(fa_p + sw128_offset(r, 2 * c));
+            const float4 a1 = *reinterpret_cast<const float4*>(fa_p + sw128_offset(r, 2 * c + 1));
+            v[0] = a0.x; v[1] = a0.y; v[2] = a0.z; v[3] = a0.w;
+            v[4] = a1.x; v[5] = a1.y; v[6] = a1.z; v[7] = a1.w;
+            uint4 o[P];
+            split8<P, SCALED>(v, ex[i], o);
+            const uint32_t off = sw64_offset(r, c);
 #pragma unroll
-            for (int p = 0; p < P; ++p) st_shared16(sa + p * S::kABytes + off, o[p]);
+            for (int p = 0; p < P; ++p) *reinterpret_cast<uint4*>(sa_p + p * S::kABytes + off) = o[p];
           } else {
             const int ub = u - S::kAUnits;
-            const uint32_t off = sw64_offset(ub % S::kHalf, ub / S::kHalf);
+            const int col = ub % S::kHalf, c = ub / S::kHalf;
+            const float* src = reinterpret_cast<const float*>(fb_p) + 8 * c * S::kHalf + col;
 #pragma unroll
-            for (int p = 0; p < P; ++p) st_shared16(sb + p * S::kBBytes + off, o[p]);
+            for (int j = 0; j < 8; ++j) v[j] = src[j * S::kHalf];
+            uint4 o[P];
+            split8<P, SCALED>(v, ex[i], o);
+            const uint32_t off = sw64_offset(col, c);
+#pragma unroll
+            for (int p = 0; p < P; ++p) *reinterpret_cast<uint4*>(sb_p + p * S::kBBytes + off) = o[p];
           }
         }
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
+          mbar_arrive(&sempty[ss]);  // the staging slot may be reloaded
           if (leader) mbar_arrive(&full[s]);
           else mbar_arrive_remote(full_leader0 + 8u * s);
         }
-        // the next k-tile's operands, possibly of the next work item: issued
-        // now, consumed one stage later
-        if (kt + 1 < w.KT) load_units(w, kt + 1);
-        else if (t + pairs < num_tiles) load_units(tiles.get(t + pairs), 0);
       }
     }
   } else {
     // ---------------- epilogue (warps 8..15, both CTAs) ----------------
+    regs_inc<kRegsHigh>();
     const int q = warp & 3;
     const int h = (warp - 8) >> 2;
     constexpr int COLS = BN / 2;

@@ -155,6 +155,22 @@ bool tc_make_parts_map_impl(CUtensorMap* map, const void* parts, int P, int rows
   return r == CUDA_SUCCESS;
 }
 
+bool tc_make_f32_map(void* map, const void* base, int inner, int outer, long ld, int box_inner,
+                     int box_outer, bool swizzle128) {
+  auto enc = get_encode();
+  if (!enc || inner <= 0 || outer <= 0) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(static_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                   const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 struct TcEntry {
   int parts, bn, stages;
   int pair;  // 1: CTA-pair kernel, 256-row tiles

@@ -36,13 +36,18 @@ def fused_ids(hb):
 
 
 def _rand(shape, seed, wide=False):
+    """Seeded operand whose row stride is a multiple of 4 floats (the fused
+    kernels read operands through FP32 TMA maps: 16-byte aligned rows); a
+    ragged column count is a view into a padded buffer."""
     import torch
     g = torch.Generator(device="cuda").manual_seed(seed)
-    x = torch.rand(shape, device="cuda", generator=g) * 2 - 1
+    rows, cols = shape
+    pad = (cols + 3) // 4 * 4
+    x = torch.rand((rows, pad), device="cuda", generator=g) * 2 - 1
     if wide:
-        u = torch.rand(shape, device="cuda", generator=g) * 40 - 20
+        u = torch.rand((rows, pad), device="cuda", generator=g) * 40 - 20
         x = torch.sign(x) * torch.exp2(u)
-    return x
+    return x[:, :cols]
 
 
 def _err(C, ref):
@@ -72,9 +77,10 @@ def test_fused_matches_unfused(hb, fused_ids, variant, bn, m, n, k):
 
 
 @pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
-def test_fused_unaligned_rows(hb, fused_ids, variant):
-    # A with a row stride that is not a multiple of 4 floats and an offset
-    # start: the converters take the 4-byte load path
+def test_fused_needs_aligned_rows(hb, fused_ids, variant):
+    # the fused kernels read A and B through FP32 TMA maps: a row stride that
+    # is not a multiple of 4 floats is rejected for an explicit fused tile
+    # (status -2) and served by the split-pass kernels otherwise
     import torch
     fused, plain = fused_ids
     P = PARTS[variant]
@@ -82,10 +88,27 @@ def test_fused_unaligned_rows(hb, fused_ids, variant):
     buf = _rand((m, k + 3), 5)
     A = buf[:, 1:k + 1]
     B = _rand((k, n), 6)
+    with pytest.raises(hb.HbsgError) as e:
+        hb.gemm(A, B, variant=variant, config={"tile": fused[(P, 256)]})
+    assert e.value.status == -2
     cfg = {"split_k": 1, "chunk_k": 64}
-    Cf = hb.gemm(A, B, variant=variant, config={**cfg, "tile": fused[(P, 256)]})
+    C = hb.gemm(A, B, variant=variant, config=cfg)
     Cu = hb.gemm(A.contiguous(), B, variant=variant, config={**cfg, "tile": plain[(P, 256)]})
+    Cf = hb.gemm(A.contiguous(), B, variant=variant, config={**cfg, "tile": fused[(P, 256)]})
     assert torch.equal(Cf, Cu)
+    ref = A.double() @ B.double()
+    assert (torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref)).item() < 2e-6
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
+def test_fused_zero_k_gives_zeros(hb, fused_ids, variant):
+    import torch
+    fused, _ = fused_ids
+    A = torch.empty((300, 0), device="cuda")
+    B = torch.empty((0, 200), device="cuda")
+    C = torch.full((300, 200), 7.0, device="cuda")
+    hb.gemm(A, B, C, variant=variant, config={"tile": fused[(PARTS[variant], 256)]})
+    assert torch.count_nonzero(C).item() == 0
 
 
 @pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
