@@ -96,6 +96,7 @@ SIGNATURES = {
     "hbsg_check_device": (_I, [_P]),
     "hbsg_debug_timeout_probe": (_I, [_P, _SZ, _P]),
     "hbsg_fp32_peak_probe": (_I, [_I, _I, _P, ctypes.POINTER(ctypes.c_double), _P]),
+    "hbsg_jacobi": (_I, [_I, _I, _P, _P, _I, _I, _I, _P]),
     "hbsg_version": (_I, []),
 }
 

@@ -771,6 +771,7 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
   gt.n = (int)L.num_tiles;
   TcRun run = pl.run;
   if (pl.fused_tile >= 0) {
+    run.l2_ahead = fused_l2_ahead();
     const int slot = scaled ? 1 : 0;
     const GFusedEntry& fe = kGFused[pl.fused_tile];
     const void* k = fe.k[slot];

@@ -83,6 +83,7 @@ int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int*
 cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sms,
                          unsigned long long wait_limit_ns, cudaStream_t st, float* partial);
 int fused_read_and_clear_device_error();
+int fused_l2_ahead();
 // Fused kernels read A and B through FP32 TMA maps: 16-byte aligned bases and
 // row strides that are multiples of 4 floats.
 bool fused_operands_ok(const float* A, long lda, const float* B, long ldb);

@@ -11,6 +11,7 @@
 // through two FP32 TMA tensor maps, so both need 16-byte aligned bases and
 // row strides (lda, ldb multiples of 4 floats).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "tc_fused.cuh"
@@ -138,6 +139,17 @@ bool fused_tile_info(int idx, hbsg_tile_info* out) {
   return true;
 }
 
+// k-tiles the loader prefetches into L2 ahead of its staging loads
+// (HBSG_FUSED_L2_AHEAD overrides the default, for tuning; 0 = off).
+int fused_l2_ahead() {
+  static const int v = [] {
+    const char* e = getenv("HBSG_FUSED_L2_AHEAD");
+    const int x = e ? atoi(e) : 0;
+    return x < 0 ? 0 : x;
+  }();
+  return v;
+}
+
 int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
   const long tiles = (long)((M + 2 * kBM - 1) / (2 * kBM)) * ((N + kFused[idx].bn - 1) / kFused[idx].bn);
   return tc_slices(tiles, K, sms / 2, requested, kt_per_split);
@@ -178,7 +190,7 @@ cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sm
   }
   TcRun run;
   run.chunk_ktiles = tc_chunk_ktiles(e.parts, chunk_k);
-  run.l2_ahead = 0;
+  run.l2_ahead = fused_l2_ahead();
   run.l2_keep = 0;
   run.debug_skip_loads = 0;
   run.wait_limit_ns = wait_limit_ns ? wait_limit_ns : kWaitLimitNs;

@@ -31,10 +31,11 @@
 //   warp 1       lane 0: TMA loads of the FP32 staging ring
 //   warps 2-7    converters (this CTA's 128 A rows and BN/2 B columns)
 //   warps 8-15   epilogue (TMEM lane quadrant warp % 4, column half)
-// Register split (setmaxnreg): warpgroups 0-1 (issuer, loader, converters,
-// which hold one 8-value unit at a time) 72 registers per thread, warpgroups
-// 2-3 (epilogue, BN/2 FP32 sums per thread) 184: 2 x 128 x 72 + 2 x 128 x 184
-// = 65536, the block's launch allotment (512 threads x 128).
+// Register split (setmaxnreg): warpgroups 0-1 (issuer, loader, converters)
+// 96 registers per thread, enough for the converters to keep about two 8-value
+// units in flight; warpgroups 2-3 (epilogue, BN/2 FP32 sums per thread) 160:
+// 2 x 128 x 96 + 2 x 128 x 160 = 65536, the block's launch allotment
+// (512 threads x 128).
 // Every wait is bounded as in the other tensor-core bodies. The TMA loads use
 // no cluster multicast: each CTA loads its own rows into its own memory.
 #pragma once
@@ -49,15 +50,15 @@ namespace hbsg {
 // shape in both: 6-product then 3-product forms, 256 then 64 columns wide.
 #define HBSG_FUSED_TILE_LIST(X) \
   X(3, 256, 2, 3)               \
-  X(2, 256, 3, 3)               \
-  X(3, 64, 3, 4)                \
-  X(2, 64, 4, 4)
+  X(2, 256, 2, 4)               \
+  X(3, 64, 3, 5)                \
+  X(2, 64, 3, 6)
 
 static constexpr int kFusedThreads = 512;
 static constexpr int kConvWarps = 6;
 static constexpr int kConvThreads = kConvWarps * 32;
-static constexpr int kRegsLow = 72;    // warpgroups 0-1
-static constexpr int kRegsHigh = 184;  // warpgroups 2-3
+static constexpr int kRegsLow = 96;    // warpgroups 0-1
+static constexpr int kRegsHigh = 160;  // warpgroups 2-3
 static_assert(2 * 128 * kRegsLow + 2 * 128 * kRegsHigh == 65536, "register split");
 
 // mbarrier probe with cluster-scope acquire: the converters of the peer CTA
@@ -81,6 +82,27 @@ HBSG_DEV bool wait_bounded_cluster(uint64_t* bar, uint32_t parity, volatile int*
   for (uint32_t i = 0;; ++i) {
     if (mbar_try_wait_cluster(bar, parity)) return true;
     if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (globaltimer() - t0 > limit_ns) {
+        *abort_flag = 1;
+        atomicExch(&g_device_error, (int)HBSG_ERR_DEVICE_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+
+// Bounded wait for roles that wait long (the epilogue waits a whole TMEM
+// drain interval): between probes the thread sleeps, so its warp does not
+// take issue slots from the converter warps sharing its scheduler.
+HBSG_DEV bool wait_bounded_sleep(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                 unsigned long long limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t i = 0;; ++i) {
+    __nanosleep(128);
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 15) == 0) {
       if (*abort_flag) return false;
       if (globaltimer() - t0 > limit_ns) {
         *abort_flag = 1;
@@ -236,6 +258,13 @@ HBSG_DEV uint32_t sw128_offset(int r, int c) {
   return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
 }
 
+HBSG_DEV void tma_prefetch_2d(const CUtensorMap* map, int c0, int c1) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1)
+               : "memory");
+}
+
 HBSG_DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
@@ -368,6 +397,10 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
         }
         const int arow = w.m0 + kBM * (int)rank;
         const int bcol = w.n0 + S::kHalf * (int)rank;
+        for (int kp = SSTAGES; kp < min(w.KT, run.l2_ahead); ++kp) {
+          tma_prefetch_2d(w.ma, (w.kt0 + kp) * kBK, arow);
+          tma_prefetch_2d(w.mb, bcol, (w.kt0 + kp) * kBK);
+        }
         for (int kt = 0; kt < w.KT; ++kt, ++it) {
           const int ss = it % SSTAGES;
           if (!wait_bounded(&sempty[ss], ((it / SSTAGES) & 1) ^ 1, abort_flag, lim)) {
@@ -379,6 +412,13 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
           mbar_arrive_expect_tx(&sfull[ss], S::kSStageBytes);
           tma_load_2d(dst, w.ma, k0, arow, &sfull[ss]);
           tma_load_2d(dst + S::kSABytes, w.mb, bcol, k0, &sfull[ss]);
+          // the k-tile l2_ahead further on, into L2 only, so that the load
+          // issued for it later finds it there (inside this work item)
+          if (run.l2_ahead > 0 && kt + run.l2_ahead < w.KT) {
+            const int kp = k0 + run.l2_ahead * kBK;
+            tma_prefetch_2d(w.ma, kp, arow);
+            tma_prefetch_2d(w.mb, bcol, kp);
+          }
         }
       }
     }
@@ -485,7 +525,7 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
       for (int c = 0; c < nchunks; ++c, ++ch) {
         const int buf = ch & 1;
         int got = 0;
-        if (lane == 0) got = wait_bounded(&tfull[buf], (ch >> 1) & 1, abort_flag, lim);
+        if (lane == 0) got = wait_bounded_sleep(&tfull[buf], (ch >> 1) & 1, abort_flag, lim);
         got = __shfl_sync(0xffffffffu, got, 0);
         if (!got) {
           ok = false;

@@ -274,3 +274,21 @@ def fp32_peak(packed: bool = True, iters: int = 4096, repeats: int = 5) -> dict:
         best = ms if best is None else min(best, ms)
     return {"tflops": flops.value / (best * 1e-3) / 1e12, "ms": best, "flops": flops.value}
 
+
+def jacobi(a0: torch.Tensor, nx: int, ny: int, nz: int, c0: int = 2, c1: int = 4,
+           out: torch.Tensor | None = None) -> torch.Tensor:
+    """One 7-point Jacobi step (the suite's apps/jacobi kernel) on a flat
+    float32 CUDA grid of nx*ny*nz elements, element (x, y, z) at
+    ((y*nx)+x)*nz + z: out = c1 * (sum of six neighbours) - c0 * a0."""
+    _check_f32_cuda("a0", a0)
+    if not a0.is_contiguous() or a0.numel() != nx * ny * nz:
+        raise ValueError("a0 must be a contiguous grid of nx*ny*nz floats")
+    if out is None:
+        out = torch.empty_like(a0)
+    _check_f32_cuda("out", out)
+    if not out.is_contiguous() or out.numel() != a0.numel():
+        raise ValueError("out must be a contiguous grid of nx*ny*nz floats")
+    with torch.cuda.device(a0.device):
+        check(lib().hbsg_jacobi(c0, c1, _ptr(a0), _ptr(out), nx, ny, nz, _stream()),
+              "hbsg_jacobi")
+    return out

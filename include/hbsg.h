@@ -233,6 +233,22 @@ int hbsg_gemm_noalloc(int trans_a, int trans_b, int m, int n, int k,
                       const float* a, int64_t lda, const float* b, int64_t ldb,
                       float* c, int64_t ldc, int variant, hbsg_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * 7-point Jacobi step, the suite's dense stencil benchmark on the same host
+ * interface.
+ *
+ * Replaces the device kernel `int kernel(int c0, int c1, float* A0,
+ * float* Anext, const int nx, const int ny, const int nz, int pod_id)`
+ * (apps/jacobi/kernel.cpp:47-143) with its enqueue (apps/jacobi/main.cpp:
+ * 95-102). A0 and Anext are caller-owned device grids of nx*ny*nz floats,
+ * element (x, y, z) at ((y*nx)+x)*nz + z, and must not overlap. Anext =
+ * c1 * (sum of the six neighbours, 0 outside the grid) - c0 * A0, with the
+ * host reference's operation order (apps/jacobi/main.cpp:19-48), so results
+ * are bit-identical to it. Asynchronous on `stream`.
+ */
+int hbsg_jacobi(int c0, int c1, const float* A0, float* Anext, int nx, int ny, int nz,
+                hbsg_stream_t stream);
+
 /* Tile-shape table for the autotuner: number of ids and their description. */
 int hbsg_num_tiles(void);
 int hbsg_tile_describe(int tile, hbsg_tile_info* out);

@@ -35,6 +35,13 @@
  *                          (apps/sgemm/main.cpp:49-52; legacy fixtures in
  *                          apps/legacy/gemm/sgemm_512/main.cpp:69-80 and
  *                          apps/legacy/gemm/sgemm_data_parallel/main.cpp:206-223).
+ *   oracle_host_jacobi     apps/jacobi/main.cpp:19-48 (host_jacobi): the
+ *                          7-point Jacobi step Anext = c1*(sum of the six
+ *                          neighbours, zero outside the grid, summed x-1, x+1,
+ *                          y-1, y+1, z-1, z+1 left to right) - c0*self, each
+ *                          product and the difference rounded separately;
+ *                          element (x, y, z) at ((y*nx)+x)*nz + z.
+ *   oracle_fill_jacobi     apps/jacobi/main.cpp:70-73: A0[i] = i % 13.
  */
 #include <math.h>
 #include <stdint.h>
@@ -222,6 +229,38 @@ void oracle_fill_identity_ramp(float* A, int M, int K, float* B, int N)
     for (long i = 0; i < (long)M * K; i++) A[i] = 0.0f;
     for (int y = 0; y < M && y < K; y++) A[(long)y * K + y] = 1.0f;
     for (long i = 0; i < (long)K * N; i++) B[i] = (float)i;
+}
+
+/* host_jacobi restated (apps/jacobi/main.cpp:19-48). */
+void oracle_host_jacobi(int c0, int c1, const float* A0, float* Anext, int nx, int ny, int nz)
+{
+    const float c0f = (float)c0;
+    const float c1f = (float)c1;
+#define HBSG_IDX(x, y, z) ((((long)(y) * nx) + (x)) * nz + (z))
+    for (int x = 0; x < nx; x++) {
+        for (int y = 0; y < ny; y++) {
+            for (int z = 0; z < nz; z++) {
+                const float self = A0[HBSG_IDX(x, y, z)];
+                const float xm1 = x > 0 ? A0[HBSG_IDX(x - 1, y, z)] : 0.0f;
+                const float xp1 = x < nx - 1 ? A0[HBSG_IDX(x + 1, y, z)] : 0.0f;
+                const float ym1 = y > 0 ? A0[HBSG_IDX(x, y - 1, z)] : 0.0f;
+                const float yp1 = y < ny - 1 ? A0[HBSG_IDX(x, y + 1, z)] : 0.0f;
+                const float zm1 = z > 0 ? A0[HBSG_IDX(x, y, z - 1)] : 0.0f;
+                const float zp1 = z < nz - 1 ? A0[HBSG_IDX(x, y, z + 1)] : 0.0f;
+                const float neighbor = xm1 + xp1 + ym1 + yp1 + zm1 + zp1;
+                const float a = c1f * neighbor;
+                const float b = c0f * self;
+                Anext[HBSG_IDX(x, y, z)] = a - b;
+            }
+        }
+    }
+#undef HBSG_IDX
+}
+
+/* apps/jacobi/main.cpp:70-73: A0[i] = i % 13. */
+void oracle_fill_jacobi(float* A0, long count)
+{
+    for (long i = 0; i < count; i++) A0[i] = (float)(i % 13);
 }
 
 int oracle_version(void) { return 1; }

@@ -10,7 +10,9 @@ Function map (reference lines each one follows are in oracle.c):
   host_mm_fma                     apps/sgemm/kernel.cpp:24-32,186-275
   gemm_f64                        FP64 product (error measurement)
   split_bf16                      FP32 -> BF16 hi/mid/lo split
+  host_jacobi                     apps/jacobi/main.cpp:19-48
   ref_host_mm                     the reference's host_mm itself (oracle/_ref)
+  ref_host_jacobi                 the reference's host_jacobi itself (oracle/_ref)
 """
 from __future__ import annotations
 
@@ -67,12 +69,33 @@ def lib():
         l.oracle_fill_mod.argtypes = [_f32p, _f32p, _L]
         l.oracle_fill_ramp_identity.argtypes = [_f32p, _f32p, _I]
         l.oracle_fill_identity_ramp.argtypes = [_f32p, _I, _I, _f32p, _I]
+        l.oracle_host_jacobi.argtypes = [_I, _I, _f32p, _f32p, _I, _I, _I]
+        l.oracle_host_jacobi.restype = None
+        l.oracle_fill_jacobi.argtypes = [_f32p, _L]
+        l.oracle_fill_jacobi.restype = None
         _lib = l
     return _lib
 
 
+_REF_JACOBI_PATH = os.path.join(_HERE, "_ref", "libref_jacobi.so")
+_ref_jacobi = None
+
+
 def ref_available() -> bool:
     return os.path.exists(_REF_PATH)
+
+
+def ref_jacobi_available() -> bool:
+    return os.path.exists(_REF_JACOBI_PATH)
+
+
+def ref_jacobi_lib():
+    global _ref_jacobi
+    if _ref_jacobi is None:
+        if not os.path.exists(_REF_JACOBI_PATH):
+            raise FileNotFoundError("reference host_jacobi library not built (oracle/_ref)")
+        _ref_jacobi = ctypes.CDLL(_REF_JACOBI_PATH)
+    return _ref_jacobi
 
 
 def ref_lib():
@@ -186,6 +209,34 @@ def fill_identity_ramp(M: int, K: int, N: int):
     b = np.empty(K * N, np.float32)
     lib().oracle_fill_identity_ramp(a, M, K, b, N)
     return a.reshape(M, K), b.reshape(K, N)
+
+
+def host_jacobi(A0: np.ndarray, nx: int, ny: int, nz: int, c0: int = 2, c1: int = 4) -> np.ndarray:
+    """host_jacobi arithmetic (apps/jacobi/main.cpp:19-48) on a flat grid of
+    nx*ny*nz floats, element (x, y, z) at ((y*nx)+x)*nz + z."""
+    a = _c32(A0).ravel()
+    assert a.size == nx * ny * nz
+    out = np.empty_like(a)
+    lib().oracle_host_jacobi(c0, c1, a, out, nx, ny, nz)
+    return out
+
+
+def fill_jacobi(count: int) -> np.ndarray:
+    a = np.empty(count, np.float32)
+    lib().oracle_fill_jacobi(a, count)
+    return a
+
+
+def ref_host_jacobi(A0: np.ndarray, nx: int, ny: int, nz: int, c0: int = 2,
+                    c1: int = 4) -> np.ndarray:
+    """Run the reference's own host_jacobi (apps/jacobi/main.cpp, oracle/_ref)."""
+    fn = getattr(ref_jacobi_lib(), "hbref_host_jacobi")
+    fn.argtypes = [_I, _I, _f32p, _f32p, _I, _I, _I]
+    fn.restype = None
+    a = _c32(A0).ravel().copy()
+    out = np.zeros_like(a)
+    fn(c0, c1, a, out, nx, ny, nz)
+    return out
 
 
 def error_vs_f64(C: np.ndarray, ref64: np.ndarray) -> dict:

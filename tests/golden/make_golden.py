@@ -14,6 +14,12 @@ Fixtures
                                 (apps/legacy/gemm/sgemm_512/main.cpp:69-80).
   sgemm_uniform_N64_NITER2.npz  seeded U[-1,1) inputs (numpy PCG64, seed 42) and
   sgemm_uniform_N128_NITER1.npz the reference host_mm outputs, per matrix.
+  jacobi_mod_64x8x512.json      the Jacobi benchmark's launch nx_64__ny_8__nz_512
+                                (apps/jacobi/tests.mk:1) on its input A0[i] = i % 13,
+                                c0 = 2, c1 = 4 (main.cpp:62-73): SHA-256 of the
+                                reference host_jacobi's output (main.cpp:19-48).
+
+    python tests/golden/make_golden.py [--jacobi]   (--jacobi: only that fixture)
 """
 import hashlib
 import json
@@ -32,8 +38,31 @@ def sha(x: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(x, np.float32).tobytes()).hexdigest()
 
 
+REFERENCE_ROOT = os.environ.get("HB_REFERENCE_ROOT", "/root/reference")
+
+
+def jacobi_fixture():
+    assert oracle.ref_jacobi_available(), "reference host_jacobi not built"
+    nx, ny, nz, c0, c1 = 64, 8, 512, 2, 4
+    a = oracle.fill_jacobi(nx * ny * nz)
+    out = oracle.ref_host_jacobi(a, nx, ny, nz, c0, c1)
+    rng = np.random.Generator(np.random.PCG64(11))
+    idx = np.sort(rng.choice(out.size, 32, replace=False))
+    with open(os.path.join(HERE, "jacobi_mod_64x8x512.json"), "w") as f:
+        json.dump({
+            "source": "reference host_jacobi (apps/jacobi/main.cpp:19-48) compiled from the reference tree",
+            "inputs": "A0[i] = i % 13 (apps/jacobi/main.cpp:70-73), c0 = 2, c1 = 4 (main.cpp:62-63)",
+            "nx": nx, "ny": ny, "nz": nz, "c0": c0, "c1": c1,
+            "sha256_anext_f32": sha(out),
+            "samples": [[int(i), float(out[i])] for i in idx],
+        }, f, indent=1)
+
+
 def main():
-    oracle.build()
+    oracle.build(REFERENCE_ROOT)
+    if "--jacobi" in sys.argv:
+        jacobi_fixture()
+        return
     assert oracle.ref_available(), "reference host_mm not built"
 
     # 1. the benchmark's own fixture, N=512 NITER=2
@@ -79,6 +108,7 @@ def main():
         assert np.array_equal(C, C0)
         np.savez_compressed(os.path.join(HERE, f"sgemm_uniform_N{n}_NITER{niter}.npz"),
                             A=A, B=B, C_ref=C, seed=np.int64(42))
+    jacobi_fixture()
     print("golden fixtures written to", HERE)
 
 

@@ -93,8 +93,10 @@ def test_fused_needs_aligned_rows(hb, fused_ids, variant):
     assert e.value.status == -2
     cfg = {"split_k": 1, "chunk_k": 64}
     C = hb.gemm(A, B, variant=variant, config=cfg)
-    Cu = hb.gemm(A.contiguous(), B, variant=variant, config={**cfg, "tile": plain[(P, 256)]})
-    Cf = hb.gemm(A.contiguous(), B, variant=variant, config={**cfg, "tile": fused[(P, 256)]})
+    Aa = torch.zeros((m, (k + 3) // 4 * 4), device="cuda")[:, :k]  # aligned rows
+    Aa.copy_(A)
+    Cu = hb.gemm(Aa, B, variant=variant, config={**cfg, "tile": plain[(P, 256)]})
+    Cf = hb.gemm(Aa, B, variant=variant, config={**cfg, "tile": fused[(P, 256)]})
     assert torch.equal(Cf, Cu)
     ref = A.double() @ B.double()
     assert (torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref)).item() < 2e-6

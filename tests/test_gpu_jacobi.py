@@ -1,0 +1,71 @@
+"""7-point Jacobi step (the suite's apps/jacobi benchmark) on the GPU through
+the C ABI, bit for bit against the host reference's arithmetic
+(oracle.host_jacobi, pinned to the reference's own host_jacobi in
+tests/test_oracle.py). The reference's registered launches
+(apps/jacobi/tests.mk:1-2) are nx x ny x nz = 64 x 8 x 512 and 32 x 8 x 512
+on the A0[i] = i % 13 fixture with c0 = 2, c1 = 4; its check is exact
+equality (apps/jacobi/main.cpp:141-150)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def hb():
+    import hb_hammerbench_b200 as hb
+    return hb
+
+
+def _run(hb, a, nx, ny, nz, c0=2, c1=4):
+    import torch
+    d = torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    return hb.jacobi(d, nx, ny, nz, c0, c1).cpu().numpy()
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(64, 8, 512), (32, 8, 512)])
+def test_reference_launches_exact(hb, oracle_mod, nx, ny, nz):
+    a = oracle_mod.fill_jacobi(nx * ny * nz)
+    assert np.array_equal(_run(hb, a, nx, ny, nz), oracle_mod.host_jacobi(a, nx, ny, nz))
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(1, 1, 1), (5, 3, 7), (33, 17, 65), (128, 40, 300),
+                                      (7, 129, 33)])
+@pytest.mark.parametrize("wide", [False, True])
+def test_random_grids_exact(hb, oracle_mod, nx, ny, nz, wide):
+    rng = np.random.Generator(np.random.PCG64(nx * 1000 + ny * 10 + nz))
+    a = rng.uniform(-1, 1, nx * ny * nz).astype(np.float32)
+    if wide:
+        a *= np.exp2(rng.uniform(-20, 20, a.size)).astype(np.float32)
+    for c0, c1 in ((2, 4), (-3, 7)):
+        assert np.array_equal(_run(hb, a, nx, ny, nz, c0, c1),
+                              oracle_mod.host_jacobi(a, nx, ny, nz, c0, c1))
+
+
+def test_large_grid_exact_sampled(hb, oracle_mod):
+    # 256^3 (64 MB): planes are independent given their neighbours, so a
+    # slab of y planes checked against the oracle on the same slab's input
+    import torch
+    nx = ny = nz = 256
+    g = torch.Generator(device="cuda").manual_seed(3)
+    a = torch.rand(nx * ny * nz, device="cuda", generator=g) * 2 - 1
+    out = hb.jacobi(a, nx, ny, nz).cpu().numpy()
+    host = a.cpu().numpy()
+    y0, y1 = 100, 104  # interior planes y0..y1-1 need planes y0-1..y1
+    slab = host[(y0 - 1) * nx * nz:(y1 + 1) * nx * nz]
+    ref = oracle_mod.host_jacobi(slab, nx, y1 - y0 + 2, nz)
+    got = out[y0 * nx * nz:y1 * nx * nz]
+    assert np.array_equal(got, ref[nx * nz:(y1 - y0 + 1) * nx * nz])
+
+
+def test_errors(hb):
+    import torch
+
+    from hb_hammerbench_b200 import _lib
+    L = _lib.lib()
+    a = torch.zeros(64, device="cuda")
+    assert L.hbsg_jacobi(2, 4, a.data_ptr(), a.data_ptr(), 4, 4, 4, None) == _lib.ERR_INVALID_ARG
+    assert L.hbsg_jacobi(2, 4, a.data_ptr(), a.data_ptr() + 32 * 4, 4, 4, 4, None) == _lib.ERR_INVALID_ARG
+    assert L.hbsg_jacobi(2, 4, None, a.data_ptr(), 4, 4, 4, None) == _lib.ERR_INVALID_ARG
+    assert L.hbsg_jacobi(2, 4, None, None, 0, 4, 4, None) == _lib.OK
+    assert L.hbsg_jacobi(2, 4, None, None, -1, 4, 4, None) == _lib.ERR_INVALID_ARG

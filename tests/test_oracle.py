@@ -126,3 +126,32 @@ def test_bf16_rounding_ties_to_even(oracle_mod):
     x = np.array([1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -(1.0 + 2.0 ** -8)], np.float32)
     hi, _, _ = oracle_mod.split_bf16(x, 0, 3)
     assert list(oracle_mod.bf16_to_f32(hi)) == [1.0, 1.0 + 2.0 ** -6, -1.0]
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(64, 8, 512), (32, 8, 512), (5, 3, 7)])
+def test_host_jacobi_matches_reference(oracle_mod, nx, ny, nz):
+    # the restatement against the reference's own host_jacobi, compiled from
+    # apps/jacobi/main.cpp: the i % 13 fixture and random floats, bit for bit
+    if not oracle_mod.ref_jacobi_available():
+        pytest.skip("reference host_jacobi library not built (no reference tree)")
+    a = oracle_mod.fill_jacobi(nx * ny * nz)
+    assert np.array_equal(oracle_mod.ref_host_jacobi(a, nx, ny, nz),
+                          oracle_mod.host_jacobi(a, nx, ny, nz))
+    rng = np.random.Generator(np.random.PCG64(nz))
+    r = rng.uniform(-1, 1, nx * ny * nz).astype(np.float32)
+    assert np.array_equal(oracle_mod.ref_host_jacobi(r, nx, ny, nz, 3, -5),
+                          oracle_mod.host_jacobi(r, nx, ny, nz, 3, -5))
+
+
+def test_jacobi_fixture_golden(oracle_mod, golden_dir):
+    # tests/golden/jacobi_mod_64x8x512.json: SHA-256 of host_jacobi's output on
+    # the reference launch nx_64__ny_8__nz_512 (made by make_golden.py from
+    # the reference's own host_jacobi)
+    import hashlib
+    import json
+    import os
+    fix = json.load(open(os.path.join(golden_dir, "jacobi_mod_64x8x512.json")))
+    nx, ny, nz = fix["nx"], fix["ny"], fix["nz"]
+    out = oracle_mod.host_jacobi(oracle_mod.fill_jacobi(nx * ny * nz), nx, ny, nz,
+                                 fix["c0"], fix["c1"])
+    assert hashlib.sha256(out.tobytes()).hexdigest() == fix["sha256_anext_f32"]
