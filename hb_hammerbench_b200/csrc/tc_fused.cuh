@@ -92,6 +92,36 @@ HBSG_DEV bool wait_bounded_cluster(uint64_t* bar, uint32_t parity, volatile int*
   }
 }
 
+// mbarrier probe that lets the hardware suspend the thread until the phase
+// completes or `ns` nanoseconds pass, so waiting warps do not spin on the
+// issue slots the converter warps need.
+HBSG_DEV bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+HBSG_DEV bool wait_bounded_hint(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                unsigned long long limit_ns) {
+  if (mbar_try_wait_hint(bar, parity, 20000)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t i = 0;; ++i) {
+    if (mbar_try_wait_hint(bar, parity, 20000)) return true;
+    if (*abort_flag) return false;
+    if (globaltimer() - t0 > limit_ns) {
+      *abort_flag = 1;
+      atomicExch(&g_device_error, (int)HBSG_ERR_DEVICE_TIMEOUT);
+      return false;
+    }
+  }
+}
+
 // Bounded wait for roles that wait long (the epilogue waits a whole TMEM
 // drain interval): between probes the thread sleeps, so its warp does not
 // take issue slots from the converter warps sharing its scheduler.
@@ -237,13 +267,22 @@ struct TcFusedShape {
   static constexpr int kAUnits = kBM * 4;
   static constexpr int kBUnits = kHalf * 4;
   static constexpr int kUnits = kAUnits + kBUnits;
-  static constexpr int kUnitsPerThread = (kUnits + kConvThreads - 1) / kConvThreads;
+  // converter warps split by operand, in proportion to the units (a B unit,
+  // eight strided loads, costs more than an A unit)
+  static constexpr int kAWarps = BN >= 128 ? kConvWarps / 2 : kConvWarps - 1;
+  static constexpr int kBWarps = kConvWarps - kAWarps;
+  static constexpr int kAThreads = 32 * kAWarps;
+  static constexpr int kBThreads = 32 * kBWarps;
+  static constexpr int kUnitsA = (kAUnits + kAThreads - 1) / kAThreads;
+  static constexpr int kUnitsB = (kBUnits + kBThreads - 1) / kBThreads;
+  static constexpr int kFullA = kAUnits / kAThreads;  // slots every A thread fills
+  static constexpr int kFullB = kBUnits / kBThreads;
   static_assert(kSmemBytes <= 232448, "shared memory");
   static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256, "pair UMMA N");
   static_assert(kBBytes % 512 == 0, "B part base keeps the 512-byte swizzle alignment");
   static_assert(kStageBytes % 1024 == 0 && kSStageBytes % 1024 == 0 && kSABytes % 1024 == 0,
                 "FP32 A staging keeps the 1024-byte alignment of the 128-byte swizzle");
-  static_assert(kAUnits % 32 == 0, "a warp's units are all A or all B");
+  static_assert(kAUnits % 32 == 0 && kHalf % 32 == 0, "a warp's units lie in 8 whole rows / 32 columns");
 };
 
 // Byte offset of the 16-byte chunk c (8 bf16) of row r in a part tile of
@@ -403,7 +442,7 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
         }
         for (int kt = 0; kt < w.KT; ++kt, ++it) {
           const int ss = it % SSTAGES;
-          if (!wait_bounded(&sempty[ss], ((it / SSTAGES) & 1) ^ 1, abort_flag, lim)) {
+          if (!wait_bounded_hint(&sempty[ss], ((it / SSTAGES) & 1) ^ 1, abort_flag, lim)) {
             ok = false;
             break;
           }
@@ -424,12 +463,18 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
     }
   } else if (warp < 8) {
     // ---------------- converters (both CTAs) ----------------
-    constexpr int NU = S::kUnitsPerThread;
-    const int cid = threadIdx.x - 64;
+    // Warps 2 .. 2+kAWarps-1 convert A rows, the others B columns, so each
+    // warp's unit loop is branch-free: all of a k-tile's loads are issued
+    // first and the units' independent split chains overlap.
     const uint32_t full_leader0 = map_to_rank(smem_u32(&full[0]), 0);
-    int ex[NU];
+    const bool a_role = warp < 2 + S::kAWarps;
+    const int tr = a_role ? threadIdx.x - 64 : threadIdx.x - 64 - 32 * S::kAWarps;
+    constexpr int NA = S::kUnitsA;   // unit slots per A thread (the last may be partial)
+    constexpr int NB = S::kUnitsB;
+    constexpr int NMAX = NA > NB ? NA : NB;
+    int ex[NMAX];
 #pragma unroll
-    for (int i = 0; i < NU; ++i) ex[i] = 0;
+    for (int i = 0; i < NMAX; ++i) ex[i] = 0;
     uint32_t it = 0;
     bool ok = true;
     for (int t = pair; t < num_tiles && ok; t += pairs) {
@@ -437,65 +482,82 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
       if constexpr (SCALED) {
         // the split exponent of each unit's row or column, fixed for the tile
 #pragma unroll
-        for (int i = 0; i < NU; ++i) {
-          const int u = cid + i * kConvThreads;
+        for (int i = 0; i < NMAX; ++i) {
           ex[i] = 0;
-          if (u < S::kAUnits) {
+          if (a_role) {
+            const int u = tr + i * S::kAThreads;
             const int m = w.m0 + kBM * (int)rank + (u >> 2);
-            if (m < w.M) ex[i] = exp_from_maxbits(w.rowmax[m]);
-          } else if (u < S::kUnits) {
-            const int n = w.n0 + S::kHalf * (int)rank + (u - S::kAUnits) % S::kHalf;
-            if (n < w.N) ex[i] = exp_from_maxbits(w.colmax[n]);
+            if (i < NA && u < S::kAUnits && m < w.M) ex[i] = exp_from_maxbits(w.rowmax[m]);
+          } else {
+            const int u = tr + i * S::kBThreads;
+            const int n = w.n0 + S::kHalf * (int)rank + u % S::kHalf;
+            if (i < NB && u < S::kBUnits && n < w.N) ex[i] = exp_from_maxbits(w.colmax[n]);
           }
         }
       }
       for (int kt = 0; kt < w.KT; ++kt, ++it) {
         const int s = it % STAGES;
         const int ss = it % SSTAGES;
-        if (!wait_bounded(&sfull[ss], (it / SSTAGES) & 1, abort_flag, lim) ||
-            !wait_bounded(&empty[s], ((it / STAGES) & 1) ^ 1, abort_flag, lim)) {
+        if (!wait_bounded_hint(&sfull[ss], (it / SSTAGES) & 1, abort_flag, lim) ||
+            !wait_bounded_hint(&empty[s], ((it / STAGES) & 1) ^ 1, abort_flag, lim)) {
           ok = false;
           break;
         }
-        const uint32_t sa = base + s * S::kStageBytes;
-        const uint32_t sb = sa + P * S::kABytes;
-        const uint32_t fa = staging + ss * S::kSStageBytes;
-        const uint32_t fb = fa + S::kSABytes;
-        // plain (non-volatile) shared-memory accesses: the compiler may
-        // overlap one unit's loads with the previous unit's arithmetic; the
-        // barrier waits above and the proxy fence below order them against
-        // the TMA writes and the tensor-core reads
-        const uint8_t* fa_p = smem + (fa - base);
-        const uint8_t* fb_p = smem + (fb - base);
-        uint8_t* sa_p = smem + (sa - base);
-        uint8_t* sb_p = smem + (sb - base);
+        // plain (non-volatile) shared-memory accesses, so the compiler can
+        // schedule them freely; the barrier waits above and the proxy fence
+        // below order them against the TMA writes and the tensor-core reads
+        const uint8_t* f_p = smem + S::kStagingOff + ss * S::kSStageBytes;
+        uint8_t* s_p = smem + s * S::kStageBytes;
+        if (a_role) {
+          float v[NA][8];
 #pragma unroll
-        for (int i = 0; i < NU; ++i) {
-          const int u = cid + i * kConvThreads;
-          if (u >= S::kUnits) continue;
-          float v[8];
-          if (u < S::kAUnits) {
-            const int r = u >> 2, c = u & 3;
-            const float4 a0 = *reinterpret_cast<const float4*>(fa_p + sw128_offset(r, 2 * c));
-            const float4 a1 = *reinterpret_cast<const float4*>(fa_p + sw128_offset(r, 2 * c + 1));
-            v[0] = a0.x; v[1] = a0.y; v[2] = a0.z; v[3] = a0.w;
-            v[4] = a1.x; v[5] = a1.y; v[6] = a1.z; v[7] = a1.w;
-            uint4 o[P];
-            split8<P, SCALED>(v, ex[i], o);
-            const uint32_t off = sw64_offset(r, c);
+          for (int i = 0; i < NA; ++i) {
+            const int u = tr + i * S::kAThreads;
+            if (i < S::kFullA || u < S::kAUnits) {
+              const int r = u >> 2, c = u & 3;
+              const float4 a0 = *reinterpret_cast<const float4*>(f_p + sw128_offset(r, 2 * c));
+              const float4 a1 = *reinterpret_cast<const float4*>(f_p + sw128_offset(r, 2 * c + 1));
+              v[i][0] = a0.x; v[i][1] = a0.y; v[i][2] = a0.z; v[i][3] = a0.w;
+              v[i][4] = a1.x; v[i][5] = a1.y; v[i][6] = a1.z; v[i][7] = a1.w;
+            }
+          }
 #pragma unroll
-            for (int p = 0; p < P; ++p) *reinterpret_cast<uint4*>(sa_p + p * S::kABytes + off) = o[p];
-          } else {
-            const int ub = u - S::kAUnits;
-            const int col = ub % S::kHalf, c = ub / S::kHalf;
-            const float* src = reinterpret_cast<const float*>(fb_p) + 8 * c * S::kHalf + col;
+          for (int i = 0; i < NA; ++i) {
+            const int u = tr + i * S::kAThreads;
+            if (i < S::kFullA || u < S::kAUnits) {
+              uint4 o[P];
+              split8<P, SCALED>(v[i], ex[i], o);
+              const uint32_t off = sw64_offset(u >> 2, u & 3);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = src[j * S::kHalf];
-            uint4 o[P];
-            split8<P, SCALED>(v, ex[i], o);
-            const uint32_t off = sw64_offset(col, c);
+              for (int p = 0; p < P; ++p)
+                *reinterpret_cast<uint4*>(s_p + p * S::kABytes + off) = o[p];
+            }
+          }
+        } else {
+          const uint8_t* fb_p = f_p + S::kSABytes;
+          uint8_t* sb_p = s_p + P * S::kABytes;
+          float v[NB][8];
 #pragma unroll
-            for (int p = 0; p < P; ++p) *reinterpret_cast<uint4*>(sb_p + p * S::kBBytes + off) = o[p];
+          for (int i = 0; i < NB; ++i) {
+            const int u = tr + i * S::kBThreads;
+            if (i < S::kFullB || u < S::kBUnits) {
+              const int col = u % S::kHalf, c = u / S::kHalf;
+              const float* src = reinterpret_cast<const float*>(fb_p) + 8 * c * S::kHalf + col;
+#pragma unroll
+              for (int j = 0; j < 8; ++j) v[i][j] = src[j * S::kHalf];
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < NB; ++i) {
+            const int u = tr + i * S::kBThreads;
+            if (i < S::kFullB || u < S::kBUnits) {
+              uint4 o[P];
+              split8<P, SCALED>(v[i], ex[i], o);
+              const uint32_t off = sw64_offset(u % S::kHalf, u / S::kHalf);
+#pragma unroll
+              for (int p = 0; p < P; ++p)
+                *reinterpret_cast<uint4*>(sb_p + p * S::kBBytes + off) = o[p];
+            }
           }
         }
         fence_proxy_async_smem();

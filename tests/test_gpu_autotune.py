@@ -44,7 +44,8 @@ def test_tune_grouped(cache):
     As = [torch.rand((m, k), device="cuda") for m, k in ((256, 320), (128, 96), (512, 64))]
     Bs = [torch.rand((k, n), device="cuda") for k, n in ((320, 192), (96, 640), (64, 256))]
     cfg = autotune.tune_grouped(As, Bs, "bf16x6", steps=1)
-    assert cfg["tile"] in (10, 11, 12)
+    x6_tiles = [t["tile"] for t in hb.tiles() if t["family"] == "bf16" and t["parts"] == 3]
+    assert cfg["tile"] in x6_tiles
     dims = [(a.shape[0], b.shape[1], a.shape[1]) for a, b in zip(As, Bs)]
     assert autotune.lookup_grouped(dims, "bf16x6") == cfg
     Cs = hb.GroupedPlan(As, Bs, variant="bf16x6", config=cfg).run()

@@ -99,7 +99,8 @@ def test_fused_needs_aligned_rows(hb, fused_ids, variant):
     Cf = hb.gemm(Aa, B, variant=variant, config={**cfg, "tile": fused[(P, 256)]})
     assert torch.equal(Cf, Cu)
     ref = A.double() @ B.double()
-    assert (torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref)).item() < 2e-6
+    bound = 2.0 ** -16 if P == 2 else 2e-6
+    assert (torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref)).item() < bound
 
 
 @pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
