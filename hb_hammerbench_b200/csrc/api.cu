@@ -104,6 +104,58 @@ struct TcChoice {
   int splits, kts;
 };
 
+// Automatic choice between the split-pass tiles and the fused-split tiles by
+// estimated time on this shape:
+//   split pass: its HBM traffic (read FP32, write the parts) plus the product
+//     at the tile's score times the tensor-core rate;
+//   fused: waves x k-tiles per work item x the measured per-k-tile cycles of
+//     the tile, at least the FP32 operands' HBM time, plus the split-K reduce.
+// The fused form is taken only when it is estimated >10 % faster. It wins
+// where the split pass is a large share: small outputs with long K (all of
+// 256 x 256 x 1048576's time is operand traffic) and tall, narrow products.
+static void tc_pick_auto(int M, int N, int K, int variant, int sms, int req, bool fusable,
+                         TcChoice* ch) {
+  constexpr double kRate = 1.6e15;  // BF16 MMA flop/s of a well-fed tile
+  constexpr double kHbm = 6.0e12;   // bytes/s of the split and product passes
+  constexpr double kClock = 1.5e9;  // SM clock under load
+  const int P = parts_of(variant);
+  const double prods = P == 3 ? 6.0 : 3.0;
+  const double flops = 2.0 * M * (double)N * K * prods;
+  const double opnds = (double)M * K + (double)K * N;
+  const double maxima = scaled_of(variant) ? opnds * 4.0 / kHbm : 0.0;
+  double score = 0.0;
+  ch->fused = false;
+  ch->idx = tc_pick_tile(M, N, K, P, sms, req, &score);
+  if (!fusable || K <= 0 || score <= 0.0) return;
+  const double t_split = opnds * (4.0 + 2.0 * P) / (0.9 * kHbm) + 6e-6;
+  const double t_unfused = t_split + flops / (kRate * score) + maxima;
+  double best = 0.0;
+  int best_idx = -1;
+  const int pairs = sms / 2;
+  for (int f = 0; f < fused_num_tiles(); ++f) {
+    if (fused_tile_parts(f) != P) continue;
+    const int bn = fused_tile_bn(f);
+    const long tiles = (long)((M + 255) / 256) * ((N + bn - 1) / bn);
+    int kts = 0;
+    const int s = fused_pick_splits(f, M, N, K, req, sms, &kts);
+    const long waves = (tiles * s + pairs - 1) / pairs;
+    const double t_conv = (double)waves * kts * fused_ktile_cycles(f) / kClock;
+    const double t_mem = opnds * 4.0 / kHbm;
+    const double t_reduce = s > 1 ? (double)s * M * N * 8.0 / kHbm : 0.0;
+    // + ~3 us per wave to fill and drain the pipeline (first staging loads,
+    // last MMAs, epilogue stores)
+    const double t = (t_conv > t_mem ? t_conv : t_mem) + 3e-6 * waves + t_reduce + maxima;
+    if (best_idx < 0 || t < best) {
+      best = t;
+      best_idx = f;
+    }
+  }
+  if (best_idx >= 0 && best < 0.9 * t_unfused) {
+    ch->fused = true;
+    ch->idx = best_idx;
+  }
+}
+
 // Tensor-core tile and K-slice count for a split-BF16 problem (shared by the
 // workspace query and the dispatcher so both agree). Returns false when an
 // explicitly requested tile does not fit the variant or the operand layout
@@ -127,7 +179,7 @@ static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg
       if (t < 0 || tc_tile_parts(t) != P) return false;
     }
   } else {
-    ch->idx = tc_pick_tile(M, N, K, P, sms, req);
+    tc_pick_auto(M, N, K, variant, sms, req, !transposed && fusable, ch);
   }
   ch->splits = ch->fused ? fused_pick_splits(ch->idx, M, N, K, req, sms, &ch->kts)
                          : tc_pick_splits(ch->idx, M, N, K, req, sms, &ch->kts);

@@ -40,7 +40,10 @@ cudaError_t split_operand_b(const float* B, long ldb, int K, int N, int Kp, int 
 int tc_num_tiles();
 bool tc_tile_info(int idx, hbsg_tile_info* out);
 int tc_tile_parts(int idx);
-int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits);
+// Best split-pass tile by score (~ the fraction of the tensor-core rate the
+// tile reaches on this shape; returned in *score_out when given).
+int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits,
+                 double* score_out = nullptr);
 cudaError_t tc_launch(int idx, const void* Ap, const void* Bp, int M, int N, int K, int Kp,
                       float* C, long ldc, const uint32_t* rowmax, const uint32_t* colmax,
                       int raster, int chunk_k, int sms, int debug_skip_loads,
@@ -84,6 +87,9 @@ cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sm
                          unsigned long long wait_limit_ns, cudaStream_t st, float* partial);
 int fused_read_and_clear_device_error();
 int fused_l2_ahead();
+// Measured SM cycles one CTA of fused entry idx spends per k-tile (the
+// converters' shared-memory traffic bounds it), for the schedule's cost model.
+double fused_ktile_cycles(int idx);
 // Fused kernels read A and B through FP32 TMA maps: 16-byte aligned bases and
 // row strides that are multiples of 4 floats.
 bool fused_operands_ok(const float* A, long lda, const float* B, long ldb);

@@ -150,6 +150,17 @@ int fused_l2_ahead() {
   return v;
 }
 
+// Per-CTA k-tile time of each entry in SM cycles at 1.5 GHz, from measured
+// kernel times on B200 (4096^3 for the 256-wide tiles, 65536x64x4096 for the
+// 64-wide ones; per-role clock64 counters put most of it in the converters):
+// the staging, split and part writes share the SM's shared memory with the
+// tensor core's operand reads, which bounds these tiles.
+double fused_ktile_cycles(int idx) {
+  const FusedEntry& e = kFused[idx];
+  if (e.bn >= 256) return e.parts == 3 ? 2450.0 : 1950.0;
+  return e.parts == 3 ? 1900.0 : 1700.0;
+}
+
 int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split) {
   const long tiles = (long)((M + 2 * kBM - 1) / (2 * kBM)) * ((N + kFused[idx].bn - 1) / kFused[idx].bn);
   return tc_slices(tiles, K, sms / 2, requested, kt_per_split);

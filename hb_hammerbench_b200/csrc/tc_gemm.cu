@@ -311,7 +311,7 @@ int tc_slices(long tiles, int K, int slots, int requested, int* kt_per_split) {
 // kMinSliceKtiles are not counted: their FP32 partials, the reduction and
 // the pipeline refill outweigh the wider tile (measured at 1024^3, 1000^3
 // and 128x128x65536: 15-30 % slower than unsliced narrow tiles).
-int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits) {
+int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits, double* score_out) {
   const int KT = ktiles_of(K);
   int best = -1;
   double best_score = -1.0;
@@ -337,6 +337,7 @@ int tc_pick_tile(int M, int N, int K, int parts, int sms, int requested_splits) 
       best = i;
     }
   }
+  if (score_out) *score_out = best_score;
   return best;
 }
 

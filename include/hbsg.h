@@ -212,10 +212,12 @@ int hbsg_gemm_grouped(int count, const hbsg_problem* problems, int variant,
  * the library: HBSG_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory that
  * every GPU which loads the library holds until the process exits.
  *
- *   - Problems whose workspace (hbsg_gemm_workspace_size with no config)
- *     exceeds HBSG_NOALLOC_SCRATCH_BYTES are rejected with
- *     HBSG_ERR_WORKSPACE before anything is launched. M = N = K = 1024 with
- *     BF16X6 needs 12.6 MB and fits.
+ *   - Problems whose workspace (hbsg_gemm_workspace_size_ex with the same
+ *     transpose flags and no config) exceeds HBSG_NOALLOC_SCRATCH_BYTES are
+ *     rejected with HBSG_ERR_WORKSPACE before anything is launched. With a
+ *     split pass, M = N = K = 1024 BF16X6 needs 12.6 MB and fits; shapes the
+ *     library serves with a fused-split tile need only the K-slice partials
+ *     and, for the scaled forms, the row and column maxima.
  *   - FFMA is rejected with HBSG_ERR_UNSUPPORTED (it needs no scratch: call
  *     hbsg_gemm).
  *   - The first call on each device looks up the array's device address

@@ -81,11 +81,13 @@ def test_noalloc_rejects_problems_beyond_the_scratch():
     import hb_hammerbench_b200 as hb
     from hb_hammerbench_b200 import _lib
     L = _lib.lib()
-    n = 2048  # BF16X6 at 2048^3 needs 50 MB of split parts > 16 MiB
+    # BF16X6 at 2048^3 with transposed operands (always served by the kernels
+    # whose split parts live in the scratch) needs 50 MB of parts > 16 MiB
+    n = 2048
     assert hb.split_layout(n, n, n, "bf16x6")["total_bytes"] > _lib.NOALLOC_SCRATCH_BYTES
     A = torch.zeros((n, n), device="cuda")
     C = torch.full((n, n), 7.0, device="cuda")
-    st = L.hbsg_gemm_noalloc(0, 0, n, n, n, _p(A), n, _p(A), n, _p(C), n, _lib.BF16X6, None)
+    st = L.hbsg_gemm_noalloc(1, 1, n, n, n, _p(A), n, _p(A), n, _p(C), n, _lib.BF16X6, None)
     assert st == _lib.ERR_WORKSPACE
     torch.cuda.synchronize()
     assert bool((C == 7.0).all())  # nothing was launched
