@@ -82,6 +82,8 @@ SIGNATURES = {
                           ctypes.POINTER(Config), _P, _SZ, _P]),
     "hbsg_gemm_workspace_size": (_SZ, [_I, _I, _I, _I, ctypes.POINTER(Config)]),
     "hbsg_gemm_workspace_size_ex": (_SZ, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Config)]),
+    "hbsg_gemm_workspace_size_for": (_SZ, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _I,
+                                           ctypes.POINTER(Config)]),
     "hbsg_get_split_layout": (_I, [_I, _I, _I, _I, ctypes.POINTER(SplitLayout)]),
     "hbsg_gemm_noalloc": (_I, [_I, _I, _I, _I, _I, _P, _I64, _P, _I64, _P, _I64, _I, _P]),
     "hbsg_grouped_workspace_size": (_SZ, [_I, ctypes.POINTER(Problem), _I, ctypes.POINTER(Config)]),

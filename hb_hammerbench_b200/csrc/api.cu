@@ -186,20 +186,42 @@ static bool tc_schedule(int M, int N, int K, int variant, const hbsg_config* cfg
   return true;
 }
 
+// fusable: 1 = the operands suit the fused-split tiles (16-byte aligned rows),
+// 0 = they do not, -1 = unknown (the size covers either schedule).
 static size_t workspace_needed(int M, int N, int K, int batch, int variant, const hbsg_config* cfg,
-                               bool transposed = false, bool fusable = true) {
+                               bool transposed = false, int fusable = -1) {
   if (variant == HBSG_FFMA) {
     const int splits = cfg && cfg->split_k > 1 ? cfg->split_k : 1;
     return ffma_workspace_bytes(M, N, batch, splits);
+  }
+  if (fusable < 0) {
+    const size_t a = workspace_needed(M, N, K, batch, variant, cfg, transposed, 1);
+    const size_t b = workspace_needed(M, N, K, batch, variant, cfg, transposed, 0);
+    return a > b ? a : b;
   }
   // The schedule (and so the split-K partial buffer) depends on the SM count
   // of the device the product will run on: sizes are for the current device.
   const int sms = current_device_sms(nullptr);
   if (sms < 0) return 0;
   TcChoice ch;
-  if (!tc_schedule(M, N, K, variant, cfg, sms, transposed, fusable, &ch)) return 0;
+  if (!tc_schedule(M, N, K, variant, cfg, sms, transposed, fusable == 1, &ch)) return 0;
   const size_t partial = ch.splits > 1 ? align256((size_t)ch.splits * M * N * 4) : 0;
   return (ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant)).total + partial;
+}
+
+// Whether gemm_dispatch may run these operands on a fused-split tile.
+static bool operands_fusable(int K, const float* A, long lda, long strideA, const float* B,
+                             long ldb, long strideB) {
+  return K == 0 ||
+         (fused_operands_ok(A, lda, B, ldb) && strideA % 4 == 0 && strideB % 4 == 0);
+}
+
+size_t gemm_workspace_exact(int trans_a, int trans_b, int m, int n, int k, const float* a,
+                            long lda, const float* b, long ldb, int variant,
+                            const hbsg_config* cfg) {
+  if (m <= 0 || n <= 0 || k < 0 || !variant_valid(variant)) return 0;
+  return workspace_needed(m, n, k, 1, variant, cfg, trans_a || trans_b,
+                          operands_fusable(k, a, lda, 0, b, ldb, 0) ? 1 : 0);
 }
 
 // Core dispatcher for one (possibly batched) GEMM.
@@ -256,10 +278,9 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   const int P = parts_of(variant);
   const bool scaled = scaled_of(variant);
   TcChoice ch;
-  // fused tiles read A and B through FP32 TMA maps (16-byte aligned rows)
-  // (with K = 0 nothing is read)
-  const bool fusable =
-      K == 0 || (fused_operands_ok(A, lda, B, ldb) && strideA % 4 == 0 && strideB % 4 == 0);
+  // fused tiles read A and B through FP32 TMA maps (16-byte aligned rows;
+  // with K = 0 nothing is read)
+  const bool fusable = operands_fusable(K, A, lda, strideA, B, ldb, strideB);
   if (!tc_schedule(M, N, K, variant, cfg, sms, trans_a || trans_b, fusable, &ch))
     return HBSG_ERR_UNSUPPORTED;
   const int tc = ch.idx, splits = ch.splits;
@@ -387,6 +408,12 @@ size_t hbsg_gemm_workspace_size_ex(int trans_a, int trans_b, int m, int n, int k
                                    const hbsg_config* cfg) {
   if (m <= 0 || n <= 0 || k < 0 || !variant_valid(variant)) return 0;
   return workspace_needed(m, n, k, 1, variant, cfg, trans_a || trans_b);
+}
+
+size_t hbsg_gemm_workspace_size_for(int trans_a, int trans_b, int m, int n, int k, const float* a,
+                                    int64_t lda, const float* b, int64_t ldb, int variant,
+                                    const hbsg_config* cfg) {
+  return gemm_workspace_exact(trans_a, trans_b, m, n, k, a, lda, b, ldb, variant, cfg);
 }
 
 int hbsg_get_split_layout(int m, int n, int k, int variant, hbsg_split_layout* out) {

@@ -107,6 +107,12 @@ int tc_slices(long tiles, int K, int slots, int requested, int* kt_per_split);
 cudaError_t maxabs_rows(const float* A, long lda, int M, int K, uint32_t* rowmax, cudaStream_t st);
 cudaError_t maxabs_cols(const float* B, long ldb, int K, int N, uint32_t* colmax, cudaStream_t st);
 
+// Workspace of one hbsg_gemm call on these operands (their alignment decides
+// whether a fused-split schedule may run).
+size_t gemm_workspace_exact(int trans_a, int trans_b, int m, int n, int k, const float* a,
+                            long lda, const float* b, long ldb, int variant,
+                            const hbsg_config* cfg);
+
 // ---- device state -------------------------------------------------------------
 // Device ordinals the per-device tables cover (one bit each in a uint64_t).
 static constexpr int kMaxDevices = 64;

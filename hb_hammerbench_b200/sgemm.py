@@ -132,8 +132,9 @@ def gemm(a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None, varian
     v = _variant(variant)
     cfgp = _config(resolve_config(m, n, k, variant, trans_a or trans_b, config))
     with torch.cuda.device(a.device):
-        need = int(lib().hbsg_gemm_workspace_size_ex(int(trans_a), int(trans_b), m, n, k, v,
-                                                     cfgp))
+        need = int(lib().hbsg_gemm_workspace_size_for(int(trans_a), int(trans_b), m, n, k,
+                                                      _ptr(a), a.stride(0), _ptr(b), b.stride(0),
+                                                      v, cfgp))
         ws = _workspace(need, a.device, workspace)
         st = lib().hbsg_gemm_ex(int(trans_a), int(trans_b), m, n, k, _ptr(a), a.stride(0),
                                 _ptr(b), b.stride(0), _ptr(c), c.stride(0), v, cfgp,

@@ -138,9 +138,16 @@ int hbsg_gemm_ex(int trans_a, int trans_b, int m, int n, int k,
 size_t hbsg_gemm_workspace_size(int m, int n, int k, int variant,
                                 const hbsg_config* cfg);
 /* The same for a call with transposed operands (the automatic schedule of a
- * transposed call never uses a fused-split tile, so its size can differ). */
+ * transposed call never uses a fused-split tile, so its size can differ).
+ * Both sizes cover either schedule the call may take: a fused-split tile needs
+ * 16-byte aligned operand rows, which these queries cannot see. */
 size_t hbsg_gemm_workspace_size_ex(int trans_a, int trans_b, int m, int n, int k, int variant,
                                    const hbsg_config* cfg);
+/* The exact workspace of a call on these operands (no reference counterpart):
+ * with aligned rows a fused-split schedule may need far less (no BF16 parts). */
+size_t hbsg_gemm_workspace_size_for(int trans_a, int trans_b, int m, int n, int k,
+                                    const float* a, int64_t lda, const float* b, int64_t ldb,
+                                    int variant, const hbsg_config* cfg);
 
 /* Where the split-BF16 path keeps the operand parts inside its workspace
  * (byte offsets from the workspace start). Parts are BF16, K-major:
@@ -212,8 +219,8 @@ int hbsg_gemm_grouped(int count, const hbsg_problem* problems, int variant,
  * the library: HBSG_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory that
  * every GPU which loads the library holds until the process exits.
  *
- *   - Problems whose workspace (hbsg_gemm_workspace_size_ex with the same
- *     transpose flags and no config) exceeds HBSG_NOALLOC_SCRATCH_BYTES are
+ *   - Problems whose workspace (hbsg_gemm_workspace_size_for on the same
+ *     operands, no config) exceeds HBSG_NOALLOC_SCRATCH_BYTES are
  *     rejected with HBSG_ERR_WORKSPACE before anything is launched. With a
  *     split pass, M = N = K = 1024 BF16X6 needs 12.6 MB and fits; shapes the
  *     library serves with a fused-split tile need only the K-slice partials

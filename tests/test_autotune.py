@@ -9,8 +9,10 @@ from hb_hammerbench_b200 import autotune, tiles
 
 @pytest.fixture
 def cache(tmp_path, monkeypatch):
+    # an empty user cache and no shipped table
     p = tmp_path / "tune.json"
     monkeypatch.setenv("HBSG_AUTOTUNE_CACHE", str(p))
+    monkeypatch.setattr(autotune, "SHIPPED_PATH", str(tmp_path / "none.json"))
     autotune.clear_memory_cache()
     yield p
     autotune.clear_memory_cache()
