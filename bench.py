@@ -361,7 +361,8 @@ def run_ours(args) -> None:
         f_steps = max(3, args.steps // 2)
         f_val = ws * flops * f_steps / (f_total * 1e-3) / 1e12
         ffma = {"value": f_val, "unit": "TFLOP/s", "ms_per_step": f_total / f_steps,
-                "error_vs_fp64": _err(C2, ref), "kernel": "ffma_sgemm_kernel (tile 1: 128x128, packed FMA)",
+                "error_vs_fp64": _err(C2, ref), "kernel": "ffma_sgemm_kernel",
+                "schedule": hb.resolve_config(n, n, n, "ffma", False, None) or "heuristic",
                 "kernel_ms": statistics.mean(f_kern)}
         del C2
     del ref
@@ -430,7 +431,9 @@ def run_ours(args) -> None:
         prods = PRODUCTS[variant]
         mma_flops = prods * flops
         achieved = mma_flops / (avg_kernel_ms * 1e-3) / 1e12
-        kname = "tc_fused_kernel" if fused else "tc_gemm_kernel"
+        tile = sched.get("tile") or 0
+        pair = bool(tile and tile_info[tile]["bm"] == 256)
+        kname = "tc_fused_kernel" if fused else ("tc_pair_kernel" if pair else "tc_gemm_kernel")
         traffic = _profile_traffic(f"{kname[:-7]}_{variant}_n{n}")
         roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
                 "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,

@@ -72,9 +72,10 @@ extern "C" int hbsg_gemm_noalloc(int trans_a, int trans_b, int m, int n, int k, 
   if (variant < HBSG_BF16X3 || variant > HBSG_BF16X6_SCALED) return HBSG_ERR_UNSUPPORTED;
   if (m < 0 || n < 0 || k < 0) return HBSG_ERR_INVALID_ARG;
   if (m == 0 || n == 0) return HBSG_OK;
+  // A fused-split schedule of an unscaled form may need no scratch at all
+  // (need == 0); argument and device errors are reported by hbsg_gemm_ex.
   const size_t need = hbsg::gemm_workspace_exact(trans_a, trans_b, m, n, k, a, lda, b, ldb, variant,
                                                  nullptr);
-  if (need == 0) return HBSG_ERR_INVALID_ARG;
   if (need > HBSG_NOALLOC_SCRATCH_BYTES) return HBSG_ERR_WORKSPACE;
   void* scratch = nullptr;
   const int s2 = hbsg::noalloc_scratch(&scratch);
