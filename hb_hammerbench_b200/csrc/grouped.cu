@@ -92,6 +92,15 @@ __global__ void __launch_bounds__(320, 1) tc_grouped_kernel(const GTiles tiles, 
   tc_body<P, BN, STAGES, SCALED>(tiles, run);
 }
 
+// CTA-pair form over 256-row tiles (tc_kernel2.cuh): the tile list holds
+// 256 x BN tiles, the A maps have 128-row boxes (each CTA loads its half of
+// the tile's rows) and the B maps BN/2-row boxes.
+template <int P, int BN, int STAGES, bool SCALED>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(320, 1)
+    tc_grouped_pair_kernel(const GTiles tiles, const TcRun run) {
+  tc_pair_body<P, BN, STAGES, SCALED>(tiles, run);
+}
+
 // Fused-split form: CTA pairs over 256-row tiles, the split done by the
 // product kernel's converter warps (tc_fused.cuh); no split pass and no parts
 // in the workspace.
@@ -638,8 +647,7 @@ static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* 
   }
   if (tile >= 0) {
     idx = tile - nf;
-    if (idx < 0 || idx >= tc_num_tiles() || tc_tile_parts(idx) != P || tc_tile_pair(idx))
-      return false;  // grouped plans run the single-CTA tiles
+    if (idx < 0 || idx >= tc_num_tiles() || tc_tile_parts(idx) != P) return false;
   } else {
     for (int i = 0; i < tc_num_tiles(); ++i)  // default: the single-CTA BN = 256 tile
       if (tc_tile_parts(i) == P && tc_tile_bn(i) == 256 && !tc_tile_pair(i)) idx = i;
@@ -690,6 +698,15 @@ struct GTcEntry {
            reinterpret_cast<const void*>(&tc_grouped_kernel<P, BN, ST, false>),          \
            reinterpret_cast<const void*>(&tc_grouped_kernel<P, BN, ST, true>)},
 static const GTcEntry kGTc[] = {HBSG_TC_TILE_LIST(HBSG_GTC_ENTRY)};
+static constexpr int kNumGTc = sizeof(kGTc) / sizeof(kGTc[0]);
+// The tensor-core table's CTA-pair entries (tc_gemm.cu), in its order after
+// the single-CTA tiles: 256 x 256 with 3 parts (4 stages), with 2 parts (6).
+#define HBSG_GTCP_ENTRY(P, BN, ST)                                                       \
+  GTcEntry{TcPairShape<P, BN, ST>::kSmemBytes,                                           \
+           reinterpret_cast<const void*>(&tc_grouped_pair_kernel<P, BN, ST, false>),     \
+           reinterpret_cast<const void*>(&tc_grouped_pair_kernel<P, BN, ST, true>)},
+static const GTcEntry kGTcPair[] = {HBSG_GTCP_ENTRY(3, 256, 4) HBSG_GTCP_ENTRY(2, 256, 6)};
+static uint64_t g_tcp_masks[2][2];
 #define HBSG_GTCI_ENTRY(P, BN, ST)                                                          \
   GTcEntry{TcShape<P, BN, ST>::kSmemBytes,                                                  \
            reinterpret_cast<const void*>(&tc_grouped_inline_kernel<P, BN, ST, false>),      \
@@ -712,6 +729,27 @@ static const GFusedEntry kGFused[] = {HBSG_FUSED_TILE_LIST(HBSG_GFUSED_ENTRY)};
 static constexpr int kNumGFused = sizeof(kGFused) / sizeof(kGFused[0]);
 static uint64_t g_fused_masks[kNumGFused][2];
 static int g_fused_regs[kNumGFused][2];
+
+// Co-resident clusters of two 320-thread CTAs of a pair kernel (0 if unknown).
+static int pair_resident_clusters(const void* kernel, int smem) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(320, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = 2;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
 
 // Launches of one grouped product on `st` (no host synchronisation, no
 // allocation: capturable).
@@ -805,6 +843,14 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
     void* args[] = {&gi, &run};
     return cudaLaunchKernel(k, dim3(pl.grid), dim3(384), args, te.smem, st);
   }
+  if (pl.tc_tile >= kNumGTc) {  // CTA pairs (cluster dimensions compiled in)
+    const int pi = pl.tc_tile - kNumGTc;
+    const GTcEntry& te = kGTcPair[pi];
+    const void* k = scaled ? te.k1 : te.k0;
+    if (!set_smem_once(k, te.smem, &g_tcp_masks[pi][scaled ? 1 : 0])) return cudaErrorInvalidValue;
+    void* args[] = {&gt, &run};
+    return cudaLaunchKernel(k, dim3(pl.grid), dim3(320), args, te.smem, st);
+  }
   const GTcEntry& te = kGTc[pl.tc_tile];
   const void* k = scaled ? te.k1 : te.k0;
   if (!set_smem_once(k, te.smem, &g_tc_masks[pl.tc_tile][scaled ? 1 : 0]))
@@ -841,11 +887,14 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
   if (!tile_shape(pl->variant, cfg, &pl->ffma_tile, &pl->tc_tile, &pl->fused_tile, &bm, &bn))
     return HBSG_ERR_UNSUPPORTED;
   const bool fused = pl->fused_tile >= 0;
+  const bool pair = pl->tc_tile >= 0 && tc_tile_pair(pl->tc_tile);
   pl->count = count;
   hbsg_config no_inline{};
   if (cfg) no_inline = *cfg;
-  no_inline.inline_split_pct = -1;  // fused plans split inside the product kernel already
-  const GSets sets = grouped_sets(count, pr, pl->variant, fused ? &no_inline : cfg);
+  // fused plans split inside the product kernel already; the CTA-pair kernel
+  // has no splitter warps
+  no_inline.inline_split_pct = -1;
+  const GSets sets = grouped_sets(count, pr, pl->variant, (fused || pair) ? &no_inline : cfg);
   pl->inline_split = sets.any_inline;
   pl->L = grouped_layout(count, pr, pl->variant, bm, bn, sets, fused);
   const GLayout& L = pl->L;
@@ -954,7 +1003,8 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
       const bool ok = fused ? fused_make_maps(pl->fused_tile, g.A, g.lda, g.B, g.ldb, g.M, g.N,
                                               g.K, &maps[2 * i], &maps[2 * i + 1])
                             : tc_make_parts_map(&maps[2 * i], g.Ap, P, g.M, g.Kp, kBM) &&
-                                  tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp, bn);
+                                  tc_make_parts_map(&maps[2 * i + 1], g.Bp, P, g.N, g.Kp,
+                                                    pair ? bn / 2 : bn);
       if (!ok) return HBSG_ERR_UNSUPPORTED;
     }
     pl->run.chunk_ktiles = tc_chunk_ktiles(P, cfg ? cfg->chunk_k : 0);
@@ -1011,6 +1061,18 @@ static int plan_build(GroupedPlan* pl, int count, const hbsg_problem* pr, const 
     pl->grid = (int)(2 * std::max<long>(1, std::min<long>(resident, L.num_tiles)));
     return HBSG_OK;
   }
+  if (pair) {
+    // pairs are dealt tiles statically: every cluster must be resident at once
+    const int pi = pl->tc_tile - kNumGTc;
+    const int slot = scaled ? 1 : 0;
+    const GTcEntry& te = kGTcPair[pi];
+    const void* k = slot ? te.k1 : te.k0;
+    if (!set_smem_once(k, te.smem, &g_tcp_masks[pi][slot])) return HBSG_ERR_LAUNCH;
+    int resident = pair_resident_clusters(k, te.smem);
+    if (resident <= 0 || resident > sms / 2) resident = sms / 2;
+    pl->grid = (int)(2 * std::max<long>(1, std::min<long>(resident, L.num_tiles)));
+    return HBSG_OK;
+  }
   const long slots = split ? sms : (long)sms * gffma_table(pl->ffma_tile).per_sm;
   pl->grid = (int)std::max<long>(1, std::min<long>(slots, L.num_tiles));
   return HBSG_OK;
@@ -1042,11 +1104,13 @@ size_t hbsg_grouped_workspace_size(int count, const hbsg_problem* problems, int 
   int fi, ti, ui, bm, bn;
   if (!tile_shape(variant, cfg, &fi, &ti, &ui, &bm, &bn)) return 0;
   const bool fused = ui >= 0;
+  const bool pair = ti >= 0 && tc_tile_pair(ti);
   hbsg_config no_inline{};
   if (cfg) no_inline = *cfg;
   no_inline.inline_split_pct = -1;
   return grouped_layout(count, problems, variant, bm, bn,
-                        grouped_sets(count, problems, variant, fused ? &no_inline : cfg),
+                        grouped_sets(count, problems, variant,
+                                     (fused || pair) ? &no_inline : cfg),
                         fused).total;
 }
 

@@ -46,6 +46,25 @@ def test_grouped_plan_matches_single(hb, variant, ragged):
     plan.close()
 
 
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3", "bf16x6_scaled", "bf16x3_scaled"])
+@pytest.mark.parametrize("ragged", [False, True])
+def test_grouped_pair_tiles_match_single(hb, variant, ragged):
+    # CTA-pair tiles (256 x 256, cta_group::2) in a grouped plan: each problem
+    # bit-identical to the single-GEMM entry point on the same pair tile
+    import torch
+    P = 3 if "x6" in variant else 2
+    tile = [t["tile"] for t in hb.tiles() if t["family"] == "bf16" and not t["fused"]
+            and t["bm"] == 256 and t["parts"] == P][0]
+    As, Bs = _problems(23 + ragged, 20, hi=700, ragged=ragged)
+    plan = hb.GroupedPlan(As, Bs, variant=variant, config={"tile": tile})
+    Cs = plan.run()
+    torch.cuda.synchronize()
+    for a, b, c in zip(As, Bs, Cs):
+        ref = hb.gemm(a, b, variant=variant, config={"tile": tile, "split_k": 1})
+        assert torch.equal(c, ref), (tuple(a.shape), tuple(b.shape))
+    plan.close()
+
+
 @pytest.mark.parametrize("variant", ["ffma", "bf16x6"])
 def test_grouped_one_shot_matches_plan(hb, variant):
     import torch
