@@ -8,10 +8,16 @@
 // output tiles of all problems form one list:
 //   - problems are ordered by K (the cost of a tile) descending, and each
 //     problem's tiles are listed in rasterised order;
-//   - CTA b of the persistent grid takes tiles b, b + G, b + 2G, ...
+//   - the CTAs of the persistent grid claim tiles in that order from a
+//     counter in the workspace (zeroed by the launch sequence before the
+//     kernel; the single-CTA tensor-core kernels hand the claimed tile to
+//     their MMA and epilogue warps through a ring in shared memory with
+//     bounded waits, tc_kernel.cuh), so a CTA that drew long tiles takes
+//     fewer and the grid ends together;
 // so the ~G tiles in flight at any moment have similar cost (balanced waves)
 // and mostly belong to one or two problems (their operand strips are shared
-// in L2).
+// in L2). The CTA-pair and fused-split kernels deal the same list statically
+// (pair p takes tiles p, p + G/2, ...).
 //
 // Split-BF16 forms: one grouped split pass over all problems writes every
 // problem's BF16 parts into the workspace; the tensor-core kernel body
@@ -52,6 +58,10 @@ struct GProblem {  // one problem, as the kernels see it
 
 struct GTiles {  // tile source for the tensor-core body (split pass run beforehand)
   static constexpr bool kInlineSplit = false;
+  // tc_body claims tiles from `queue` (zeroed before each launch); the pair
+  // and fused-split bodies deal them statically
+  static constexpr bool kQueue = true;
+  int* queue;
   __device__ bool wait_ready(int, int, volatile int*, unsigned long long) const { return true; }
   template <int P, bool SCALED>
   __device__ void split_worker(int, volatile int*) const {}
@@ -353,15 +363,27 @@ __global__ void __launch_bounds__(384, 1)
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool VEC, bool PAIR>
 __global__ void __launch_bounds__(FfmaShape<BM, BN, BK, WM, WN, STAGES>::kThreads,
                                   FfmaShape<BM, BN, BK, WM, WN, STAGES>::kMinBlocks)
-    ffma_grouped_kernel(const GProblem* __restrict__ probs, const int4* __restrict__ tiles, int n) {
+    ffma_grouped_kernel(const GProblem* __restrict__ probs, const int4* __restrict__ tiles, int n,
+                        int* __restrict__ queue) {
+  // Tiles are claimed from `queue` (zeroed before the launch): thread 0 claims
+  // the next tile when a tile starts, so the atomic's latency overlaps it.
   extern __shared__ __align__(16) float smem[];
-  for (int t = blockIdx.x; t < n; t += gridDim.x) {
+  __shared__ int s_next;
+  if (threadIdx.x == 0) s_next = atomicAdd(queue, 1);
+  __syncthreads();
+  int t = s_next;
+  while (t < n) {
+    int nxt = 0;
+    if (threadIdx.x == 0) nxt = atomicAdd(queue, 1);
     const int4 e = tiles[t];
     const GProblem& p = probs[e.x];
     const bool vec_store = ((p.ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
-    __syncthreads();  // the previous tile's last reads of the ring are done
     ffma_tile<BM, BN, BK, WM, WN, STAGES, VEC, PAIR>(p.A, p.lda, p.B, p.ldb, p.M, p.N, 0, p.K,
                                                      e.y, e.z, p.C, p.ldc, vec_store, smem);
+    __syncthreads();  // the tile's last reads of the ring and of s_next are done
+    if (threadIdx.x == 0) s_next = nxt;
+    __syncthreads();
+    t = s_next;
   }
 }
 
@@ -492,7 +514,7 @@ static int parts_of_v(int v) { return (v == HBSG_BF16X6 || v == HBSG_BF16X6_SCAL
 static bool scaled_of_v(int v) { return v == HBSG_BF16X3_SCALED || v == HBSG_BF16X6_SCALED; }
 
 struct GLayout {
-  size_t probs_off, tiles_off, maps_off, jobs_off, sync_off, parts_off, max_off, total;
+  size_t probs_off, tiles_off, maps_off, jobs_off, queue_off, sync_off, parts_off, max_off, total;
   long num_tiles, num_jobs_a, num_jobs_b, num_jobs_rmax, num_jobs_cmax;
   long inline_jobs;  // 32 x 32 split jobs of the inline split (0 when split separately)
   size_t colmax_bytes;
@@ -606,7 +628,8 @@ static GLayout grouped_layout(int count, const hbsg_problem* pr, int variant, in
   // FP32 operands
   L.jobs_off = al(L.maps_off + (split ? sizeof(CUtensorMap) * 2 * (size_t)count : 0), 256);
   const long jobs = L.num_jobs_a + L.num_jobs_b + L.num_jobs_rmax + L.num_jobs_cmax;
-  L.sync_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);
+  L.queue_off = al(L.jobs_off + sizeof(int4) * (size_t)jobs, 256);  // tile queue counter
+  L.sync_off = L.queue_off + 256;
   L.sync_bytes = inline_split ? al(sizeof(int) * ((size_t)count + 1), 256) : 0;
   const size_t sync_tables = inline_split ? al(sizeof(int) * (3 * (size_t)count + 1), 256) : 0;
   L.parts_off = al(L.sync_off + L.sync_bytes + sync_tables, 256);
@@ -764,7 +787,10 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
     if (!set_smem_once(k, e.smem, &g_ffma_masks[pl.ffma_tile][pl.vec ? 0 : 1]))
       return cudaErrorInvalidValue;
     int n = (int)L.num_tiles;
-    void* args[] = {&probs, &tiles, &n};
+    int* queue = reinterpret_cast<int*>(pl.ws + L.queue_off);
+    cudaError_t qe = cudaMemsetAsync(queue, 0, sizeof(int), st);
+    if (qe != cudaSuccess) return qe;
+    void* args[] = {&probs, &tiles, &n, &queue};
     return cudaLaunchKernel(k, dim3(pl.grid), dim3(e.threads), args, e.smem, st);
   }
   const int P = parts_of_v(pl.variant);
@@ -803,6 +829,9 @@ static cudaError_t grouped_launch(const GroupedPlan& pl, cudaStream_t st) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   GTiles gt;
+  gt.queue = reinterpret_cast<int*>(pl.ws + L.queue_off);
+  e = cudaMemsetAsync(gt.queue, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
   gt.probs = probs;
   gt.tiles = tiles;
   gt.maps = reinterpret_cast<const CUtensorMap*>(pl.ws + L.maps_off);

@@ -50,6 +50,7 @@ struct TcParams {
 // strips in L2.
 struct SingleTiles {
   static constexpr bool kInlineSplit = false;
+  static constexpr bool kQueue = false;  // tiles dealt statically (all the same size)
   __device__ bool wait_ready(int, int, volatile int*, unsigned long long) const { return true; }
   template <int P, bool SCALED>
   __device__ void split_worker(int, volatile int*) const {}

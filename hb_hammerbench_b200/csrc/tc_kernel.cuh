@@ -32,6 +32,7 @@ static __device__ int g_device_error = 0;
   X(2, 192, 5)
 
 static constexpr int kBM = 128;
+static constexpr int kTileQueue = 8;  // entries of the tile queue ring in shared memory
 static constexpr int kBK = 32;  // bf16 elements per k-tile row = 64 bytes = one swizzle row
 static constexpr unsigned long long kWaitLimitNs = 4000000000ull;  // default bound: 4 s
 
@@ -177,7 +178,10 @@ struct TcShape {
   static constexpr int kAllocCols = kTmemCols <= 32 ? 32 : kTmemCols <= 64 ? 64 : kTmemCols <= 128 ? 128 : kTmemCols <= 256 ? 256 : 512;
   static constexpr int kBarBytes = 8 * (2 * STAGES + 4) + 16;
   static constexpr int kColExpBytes = 8 * 4 * (BN / 2);  // scaled epilogue: per-warp column exponents
-  static constexpr int kSmemBytes = 1024 + STAGES * kStageBytes + kBarBytes + kColExpBytes;
+  // tile queue (grouped launches): kTileQueue barrier pairs, then the entries
+  static constexpr int kQueueOff = STAGES * kStageBytes + kBarBytes + kColExpBytes;
+  static constexpr int kQueueBytes = kTileQueue * (2 * 8 + 16);
+  static constexpr int kSmemBytes = 1024 + kQueueOff + kQueueBytes;
   static constexpr int kThreads = 320;
   static_assert(kSmemBytes <= 232448, "shared memory");
   static_assert(BN % 16 == 0 && BN >= 64 && BN <= 256, "UMMA N");
@@ -300,7 +304,15 @@ HBSG_DEV void store_rows_transposed(float* sum, const TileWork& w, int row0, int
 }
 
 // Kernel body shared by the single-GEMM and grouped launches. `Tiles` gives
-// count() and get(t); CTA b processes tiles b, b + gridDim.x, ...
+// count() and get(t). Tiles are dealt in one of two ways:
+//   - Tiles::kQueue false: CTA b processes tiles b, b + gridDim.x, ...
+//   - Tiles::kQueue true (grouped launches): the producer thread claims the
+//     next tile from a global counter (tiles.queue, zeroed before the launch)
+//     one tile ahead, and hands each claimed tile (index, k-tiles, MMA width)
+//     to the MMA issuer and the epilogue through a ring of kTileQueue entries
+//     in shared memory (full / empty mbarrier pairs, every wait bounded); an
+//     index of -1 ends the sequence. A CTA that drew long tiles then takes
+//     fewer, so the persistent grid ends together however uneven the tiles.
 // When Tiles::kInlineSplit is true the CTA has two more warps (10, 11) that
 // produce the BF16 operand parts while the tensor cores work
 // (Tiles::split_worker), and the producer waits for a problem's parts to be
@@ -320,6 +332,9 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   int* col_exp = reinterpret_cast<int*>(smem + STAGES * S::kStageBytes + S::kBarBytes);
+  uint64_t* qfull = reinterpret_cast<uint64_t*>(smem + S::kQueueOff);  // producer published
+  uint64_t* qempty = qfull + kTileQueue;  // the MMA issuer and the 8 epilogue warps read it
+  volatile int* qent = reinterpret_cast<volatile int*>(qempty + kTileQueue);  // 4 ints an entry
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -333,6 +348,10 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 8);
+    }
+    for (int j = 0; j < kTileQueue; ++j) {
+      mbar_init(&qfull[j], 1);
+      mbar_init(&qempty[j], 9);
     }
     *abort_flag = 0;
     fence_barrier_init();
@@ -349,22 +368,57 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
   const uint32_t tmem_base = *tmem_slot;
   const unsigned long long lim = run.wait_limit_ns;
 
+  // Next entry of the tile queue for a consumer (the MMA issuer, or lane 0 of
+  // an epilogue warp): {tile or -1, k-tiles, MMA width}; false on abort.
+  auto queue_take = [&](uint32_t& q, int4& e) -> bool {
+    const int j = (int)(q % kTileQueue);
+    if (!wait_bounded(&qfull[j], (q / kTileQueue) & 1, abort_flag, lim)) return false;
+    e = make_int4(qent[4 * j], qent[4 * j + 1], qent[4 * j + 2], 0);
+    mbar_arrive(&qempty[j]);
+    ++q;
+    return true;
+  };
+
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
-      uint32_t it = 0;
+      uint32_t it = 0, q = 0;
       bool ok = true;
       const CUtensorMap* last_ma = nullptr;
       int ready_prob = -1;
       const uint64_t keep = l2_policy_evict_last();
+      // the current tile t and the next tn are known (claimed) one tile
+      // ahead, so the description loads and the claim's atomic never sit on
+      // the critical path at a tile switch
+      int t, tn;
+      if constexpr (Tiles::kQueue) {
+        t = atomicAdd(tiles.queue, 1);
+        tn = t < num_tiles ? atomicAdd(tiles.queue, 1) : num_tiles;
+      } else {
+        t = blockIdx.x;
+        tn = t + (int)gridDim.x;
+      }
       TileWork w;
-      if (blockIdx.x < num_tiles) w = tiles.get(blockIdx.x);
-      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        // the next tile's description is fetched one tile ahead, so its
-        // global loads never sit on the critical path at a tile switch
+      if (t < num_tiles) w = tiles.get(t);
+      for (;;) {
+        if constexpr (Tiles::kQueue) {
+          // publish t (or the end of the sequence) to the consumers
+          const int j = (int)(q % kTileQueue);
+          if (!wait_bounded(&qempty[j], ((q / kTileQueue) & 1) ^ 1, abort_flag, lim)) {
+            ok = false;
+            break;
+          }
+          const int nv = t < num_tiles ? min(BN, w.N - w.n0) : 0;
+          qent[4 * j] = t < num_tiles ? t : -1;
+          qent[4 * j + 1] = t < num_tiles ? w.KT : 0;
+          qent[4 * j + 2] = nv;
+          mbar_arrive(&qfull[j]);
+          ++q;
+        }
+        if (t >= num_tiles || !ok) break;
         TileWork nx = w;
-        const bool has_next = t + (int)gridDim.x < num_tiles;
-        if (has_next) nx = tiles.get(t + gridDim.x);
+        const bool has_next = tn < num_tiles;
+        if (has_next) nx = tiles.get(tn);
         if constexpr (Tiles::kInlineSplit) {
           if (w.ready_target > 0 && w.prob != ready_prob) {
             if (!tiles.wait_ready(w.prob, w.ready_target, abort_flag, lim)) {
@@ -415,23 +469,45 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(nx.mb)) : "memory");
           }
         }
+        if (!ok) break;
         w = nx;
+        t = tn;
+        if constexpr (Tiles::kQueue) {
+          if (tn < num_tiles) tn = atomicAdd(tiles.queue, 1);
+        } else {
+          tn += (int)gridDim.x;
+        }
       }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      uint32_t it = 0, ch = 0;
+      uint32_t it = 0, ch = 0, q = 0;
       bool ok = true;
-      TileWork w;
-      if (blockIdx.x < num_tiles) w = tiles.get(blockIdx.x);
-      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        TileWork nx = w;  // fetched one tile ahead (see the producer)
-        if (t + (int)gridDim.x < num_tiles) nx = tiles.get(t + gridDim.x);
-        const int KT = w.KT;
+      int t = blockIdx.x;
+      TileWork w;  // static deal: fetched one tile ahead (see the producer)
+      if constexpr (!Tiles::kQueue) {
+        if (t < num_tiles) w = tiles.get(t);
+      }
+      for (;;) {
+        int KT, nv;
+        if constexpr (Tiles::kQueue) {
+          int4 e;
+          if (!queue_take(q, e)) break;
+          if (e.x < 0) break;
+          KT = e.y;
+          nv = e.z;
+        } else {
+          if (t >= num_tiles) break;
+          TileWork nx = w;
+          if (t + (int)gridDim.x < num_tiles) nx = tiles.get(t + gridDim.x);
+          KT = w.KT;
+          nv = min(BN, w.N - w.n0);
+          w = nx;
+          t += gridDim.x;
+        }
         // MMA width trimmed to the tile's valid columns (multiple of 16): the
         // last column tile of a problem does no tensor work on padding.
-        const int nv = min(BN, w.N - w.n0);
         const uint32_t idesc = f16_idesc(kBM, nv >= BN ? BN : ((nv + 15) & ~15));
         const int nchunks = (KT + run.chunk_ktiles - 1) / run.chunk_ktiles;
         int kt = 0;
@@ -457,9 +533,9 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
 #pragma unroll
             for (int ks = 0; ks < kBK / 16; ++ks) {
 #pragma unroll
-              for (int q = 0; q < Products<P>::n; ++q) {
-                const uint64_t ad = sw64_desc(sa + Products<P>::a(q) * S::kABytes + ks * 32);
-                const uint64_t bd = sw64_desc(sb + Products<P>::b(q) * S::kBBytes + ks * 32);
+              for (int q2 = 0; q2 < Products<P>::n; ++q2) {
+                const uint64_t ad = sw64_desc(sa + Products<P>::a(q2) * S::kABytes + ks * 32);
+                const uint64_t bd = sw64_desc(sb + Products<P>::b(q2) * S::kBBytes + ks * 32);
                 tc_mma(d, ad, bd, idesc, first ? 0u : 1u);
                 first = false;
               }
@@ -468,7 +544,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           }
           if (ok) tc_commit(&tfull[buf]);
         }
-        w = nx;
+        if (!ok) break;
       }
     }
   } else if (warp >= 10) {
@@ -479,10 +555,21 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
     const int q = warp & 3;         // TMEM lane quadrant this warp may access
     const int h = (warp - 2) >> 2;  // column half
     constexpr int COLS = BN / 2;
-    uint32_t ch = 0;
+    uint32_t ch = 0, qs = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+    int t = blockIdx.x;
+    for (;;) {
+      if constexpr (Tiles::kQueue) {
+        int4 e = make_int4(-1, 0, 0, 0);
+        int got = 1;
+        if (lane == 0) got = queue_take(qs, e);
+        t = __shfl_sync(0xffffffffu, got ? e.x : -2, 0);
+        if (t < 0) break;  // -1: end of the sequence; -2: abort
+      } else {
+        if (t >= num_tiles) break;
+      }
       const TileWork w = tiles.get(t);
+      if constexpr (!Tiles::kQueue) t += gridDim.x;
       const int nchunks = (w.KT + run.chunk_ktiles - 1) / run.chunk_ktiles;
       float sum[COLS];
 #pragma unroll
