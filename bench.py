@@ -520,6 +520,12 @@ LEGS = [
 ]
 
 
+BS_LEGS = [
+    ("blackscholes_10M_records", "num-option_10000000"),
+    ("blackscholes_10M_arrays", "num-option_10000000__LAYOUT_arrays"),
+]
+
+
 def _config_legs(hb, peaks: dict, fp32_tflops: float, single_x6: float, single_ffma) -> dict:
     """Each leg: effective TFLOP/s of the whole step (split passes included),
     its error vs FP64, and the fraction of its roof: the lower of the compute
@@ -553,6 +559,18 @@ def _config_legs(hb, peaks: dict, fp32_tflops: float, single_x6: float, single_f
             if single:
                 leg["ratio_to_single_8192"] = r["tflops"] / single
         out[key] = leg
+        torch.cuda.empty_cache()
+    # Black-Scholes (apps/blackscholes) at the size of the benchmark's input
+    # file, 10 M options, on both layouts: HBM-bound, so the roof is the
+    # measured copy bandwidth over the layout's DRAM bytes per option.
+    for key, case in BS_LEGS:
+        r = sweep.run_case(case, steps=20, warmup=3)
+        out[key] = {"case": case, "value": r["moptions_per_s"], "unit": "Moptions/s",
+                    "ms_per_step": r["ms"], "changed_after_repeat": r["changed_after_repeat"],
+                    "roofline": {"bound": "hbm", "achieved": r["dram_gbs"],
+                                 "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                 "frac": r["dram_gbs"] / peaks["hbm_gbs"],
+                                 "bytes_per_option": r["bytes_per_option"]}}
         torch.cuda.empty_cache()
     return out
 

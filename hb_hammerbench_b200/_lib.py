@@ -99,6 +99,8 @@ SIGNATURES = {
     "hbsg_debug_timeout_probe": (_I, [_P, _SZ, _P]),
     "hbsg_fp32_peak_probe": (_I, [_I, _I, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "hbsg_jacobi": (_I, [_I, _I, _P, _P, _I, _I, _I, _P]),
+    "hbsg_blackscholes": (_I, [_P, ctypes.c_int64, _P]),
+    "hbsg_blackscholes_arrays": (_I, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, _P]),
     "hbsg_version": (_I, []),
 }
 

@@ -16,16 +16,23 @@ KEY_value fields. Recognised keys:
   DIST_<d>                   uniform (U[-1,1), default) | wide (sign * 2^u, u ~ U[-20,20])
   SPLITK_<s> / TILE_<t> / CHUNK_<c>
                              explicit schedule (hbsg_config.split_k / .tile / .chunk_k)
+  num-option_<n>             Black-Scholes (apps/blackscholes/tests.mk:1): n seeded
+                             synthetic option records priced in place
+  LAYOUT_<l>                 Black-Scholes layout: records (default) | arrays
 
 Examples: N_512__NITER_2, N_8192__NITER_1__V_bf16x6, M_256__N_256__K_1048576__V_bf16x6,
-GROUPED_512__SEED_0__V_bf16x6, N_8192__NITER_1__V_bf16x6_scaled__DIST_wide.
+GROUPED_512__SEED_0__V_bf16x6, N_8192__NITER_1__V_bf16x6_scaled__DIST_wide,
+num-option_32768, num-option_10000000__LAYOUT_arrays.
 
 Each case prints one JSON line: effective TFLOP/s (sum of 2*M*N*K over the
 step time, CUDA events over the timed steps), and unless --no-error the
 max-abs and relative Frobenius error of the result against an FP64 product
 of the same inputs (torch float64 matmul on the GPU). Inputs are seeded and
 generated on the device. --profile runs warm-up and timed steps only (for
-Nsight Compute).
+Nsight Compute). Black-Scholes cases print options per second and the DRAM
+bytes per second of the layout (records: the 32-byte record read and written
+back, 64 bytes per option; arrays: 20 bytes read and 8 written), and instead
+of the FP64 error the count of options that differ from the first step.
 """
 from __future__ import annotations
 
@@ -52,7 +59,7 @@ def parse_case(name: str) -> dict:
         out[key.upper()] = int(val) if val.lstrip("-").isdigit() else val.lower()
     if "V" in out and out["V"] not in VARIANTS:
         raise ValueError(f"unknown variant {out['V']!r}")
-    if "GROUPED" not in out and "N" not in out:
+    if "GROUPED" not in out and "N" not in out and "NUM-OPTION" not in out:
         raise ValueError(f"case {name!r} names no problem size")
     return out
 
@@ -91,9 +98,65 @@ def _config(c: dict):
     return cfg or None
 
 
+BS_LAYOUT_BYTES = {"records": 64, "arrays": 28}  # DRAM bytes per option
+
+
+def _timed(step, steps: int, warmup: int) -> float:
+    """Mean ms per step over `steps` steps after `warmup`, CUDA events on the
+    current stream."""
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_blackscholes(name: str, steps: int = 10, warmup: int = 3, check: bool = True,
+                     device=None) -> dict:
+    from . import blackscholes as bs
+    c = parse_case(name)
+    n = c["NUM-OPTION"]
+    layout = c.get("LAYOUT", "records")
+    if layout not in BS_LAYOUT_BYTES:
+        raise ValueError(f"unknown layout {layout!r}")
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    rec = torch.from_numpy(bs.option_records(n, c.get("SEED", 0))).to(device)
+    if layout == "records":
+        def step():
+            bs.price(rec)
+        outputs = lambda: rec[:, 5:7].clone()  # noqa: E731
+    else:
+        cols = [rec[:, j].contiguous() for j in range(5)]
+        call, put = torch.empty_like(cols[0]), torch.empty_like(cols[0])
+
+        def step():
+            bs.price_arrays(*cols, call=call, put=put)
+        outputs = lambda: torch.stack([call, put], 1)  # noqa: E731
+    step()
+    torch.cuda.synchronize()
+    first = outputs()
+    ms = _timed(step, steps, warmup)
+    res = {"case": name, "layout": layout, "options": n, "ms": ms,
+           "moptions_per_s": n / (ms * 1e-3) / 1e6,
+           "dram_gbs": n * BS_LAYOUT_BYTES[layout] / (ms * 1e-3) / 1e9,
+           "bytes_per_option": BS_LAYOUT_BYTES[layout]}
+    if check:
+        res["changed_after_repeat"] = int((outputs() != first).any(1).sum())
+    return res
+
+
 def run_case(name: str, steps: int = 10, warmup: int = 3, error: bool = True,
              profile: bool = False, device=None) -> dict:
     c = parse_case(name)
+    if "NUM-OPTION" in c:
+        return run_blackscholes(name, steps, warmup, error and not profile, device)
     device = device or torch.device("cuda", torch.cuda.current_device())
     variant = c.get("V", "ffma")
     dist = c.get("DIST", "uniform")

@@ -258,6 +258,49 @@ int hbsg_gemm_noalloc(int trans_a, int trans_b, int m, int n, int k,
 int hbsg_jacobi(int c0, int c1, const float* A0, float* Anext, int nx, int ny, int nz,
                 hbsg_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Black-Scholes European option pricing, the suite's apps/blackscholes
+ * benchmark on the same host interface.
+ *
+ * hbsg_option has the layout of the reference's OptionData
+ * (apps/blackscholes/option_data.hpp:2-13), so an array of those records
+ * binds directly. Prices are the device kernel's arithmetic
+ * (BlkSchlsEqEuroNoDiv_kernel, apps/blackscholes/bs_kernel.hpp:163-198):
+ * Taylor-series ln and exp and Hull's cumulative normal, every step the same
+ * IEEE operation, so results are bit-identical to that kernel; against the
+ * host reference (bs.hpp:60-125, libm exp/log) they stay inside the
+ * testbench's bound (sum of squared call and put differences <= 0.01 over
+ * its 32768 options, main.cpp:119-141). Inputs are meant for the range that
+ * kernel was written for (s / strike near 1, as in the benchmark's input).
+ */
+typedef struct hbsg_option {
+    float s;      /* spot price */
+    float strike; /* strike price */
+    float r;      /* risk-free interest rate */
+    float v;      /* volatility */
+    float t;      /* time to maturity in years */
+    float call;   /* output: call price */
+    float put;    /* output: put price */
+    float unused;
+} hbsg_option;
+
+/* Replaces the device kernel `int kernel(OptionData* data, int num_option,
+ * int pod_id)` (apps/blackscholes/kernel.cpp:27-113) with its enqueue
+ * (apps/blackscholes/main.cpp:79-90): prices num_option records of the
+ * caller-owned device array `options` in place, writing call and put only.
+ * Any num_option >= 0 (the reference kernel needs a multiple of its chunk of
+ * 4). Asynchronous on `stream`. */
+int hbsg_blackscholes(hbsg_option* options, int64_t num_option, hbsg_stream_t stream);
+
+/* The same pricing on separate device arrays of n floats (28 bytes per
+ * option instead of the record's 32 read and 32 written): call[i], put[i]
+ * from s[i], strike[i], r[i], v[i], t[i]. call and put must not overlap each
+ * other or any input. No counterpart in the reference (its records are the
+ * only layout); bit-identical to hbsg_blackscholes on the same values. */
+int hbsg_blackscholes_arrays(const float* s, const float* strike, const float* r,
+                             const float* v, const float* t, float* call, float* put,
+                             int64_t n, hbsg_stream_t stream);
+
 /* Tile-shape table for the autotuner: number of ids and their description. */
 int hbsg_num_tiles(void);
 int hbsg_tile_describe(int tile, hbsg_tile_info* out);

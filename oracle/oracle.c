@@ -42,6 +42,20 @@
  *                          product and the difference rounded separately;
  *                          element (x, y, z) at ((y*nx)+x)*nz + z.
  *   oracle_fill_jacobi     apps/jacobi/main.cpp:70-73: A0[i] = i % 13.
+ *   oracle_bs_host         apps/blackscholes/bs.hpp:5-125 (CNDF,
+ *                          BlkSchlsEqEuroNoDiv): the host reference the
+ *                          testbench validates against (main.cpp:109-141),
+ *                          with the C library's expf, logf and sqrt.
+ *   oracle_bs_device       apps/blackscholes/bs_kernel.hpp:33-198 (my_logf,
+ *                          expf_0, fast_expf, dual_CNDF,
+ *                          BlkSchlsEqEuroNoDiv_kernel): the device kernel's
+ *                          own arithmetic, built only from IEEE operations.
+ *                          Each fmadd_asm / fnmsub_asm is one fmaf; every
+ *                          other product, sum, quotient and square root is
+ *                          rounded on its own (the device build is ISO
+ *                          C++14 with no contraction of plain expressions).
+ *   Both work in place on option records of 8 floats (option_data.hpp:2-13:
+ *   s, strike, r, v, t, call, put, unused), writing call and put only.
  */
 #include <math.h>
 #include <stdint.h>
@@ -261,6 +275,152 @@ void oracle_host_jacobi(int c0, int c1, const float* A0, float* Anext, int nx, i
 void oracle_fill_jacobi(float* A0, long count)
 {
     for (long i = 0; i < count; i++) A0[i] = (float)(i % 13);
+}
+
+/* ---- Black-Scholes (apps/blackscholes) ---------------------------------- */
+
+enum { BS_S = 0, BS_STRIKE = 1, BS_R = 2, BS_V = 3, BS_T = 4, BS_CALL = 5, BS_PUT = 6, BS_REC = 8 };
+
+/* CNDF restated (bs.hpp:6-58): Hull's polynomial approximation of the
+ * cumulative normal, with expf from the C library. */
+static float bs_host_cndf(float InputX)
+{
+    int sign = 0;
+    if (InputX < 0.0f) {
+        InputX = -InputX;
+        sign = 1;
+    }
+    const float xInput = InputX;
+    const float expValues = expf(-0.5f * InputX * InputX);
+    const float xNPrimeofX = expValues * 0.39894228040143270286f;
+    float xK2 = 0.2316419f * xInput;
+    xK2 = 1.0f + xK2;
+    xK2 = 1.0f / xK2;
+    const float xK2_2 = xK2 * xK2;
+    const float xK2_3 = xK2_2 * xK2;
+    const float xK2_4 = xK2_3 * xK2;
+    const float xK2_5 = xK2_4 * xK2;
+    float xLocal_1 = xK2 * 0.319381530f;
+    float xLocal_2 = xK2_2 * (-0.356563782f);
+    float xLocal_3 = xK2_3 * 1.781477937f;
+    xLocal_2 = xLocal_2 + xLocal_3;
+    xLocal_3 = xK2_4 * (-1.821255978f);
+    xLocal_2 = xLocal_2 + xLocal_3;
+    xLocal_3 = xK2_5 * 1.330274429f;
+    xLocal_2 = xLocal_2 + xLocal_3;
+    xLocal_1 = xLocal_2 + xLocal_1;
+    float xLocal = xLocal_1 * xNPrimeofX;
+    xLocal = 1.0f - xLocal;
+    return sign ? 1.0f - xLocal : xLocal;
+}
+
+/* BlkSchlsEqEuroNoDiv restated (bs.hpp:60-125), n records in place. */
+void oracle_bs_host(float* data, long n)
+{
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        float* o = data + i * BS_REC;
+        const float s = o[BS_S], k = o[BS_STRIKE], r = o[BS_R], v = o[BS_V], t = o[BS_T];
+        const float sqrt_t = sqrtf(t);
+        const float logValues = logf(s / k);
+        float xPowerTerm = v * v;
+        xPowerTerm = xPowerTerm * 0.5f;
+        float xD1 = r + xPowerTerm;
+        xD1 = xD1 * t;
+        xD1 = xD1 + logValues;
+        const float xDen = v * sqrt_t;
+        xD1 = xD1 / xDen;
+        const float xD2 = xD1 - xDen;
+        const float NofXd1 = bs_host_cndf(xD1);
+        const float NofXd2 = bs_host_cndf(xD2);
+        const float FutureValueX = k * expf(-r * t);
+        o[BS_CALL] = (s * NofXd1) - (FutureValueX * NofXd2);
+        const float NegNofXd1 = 1.0f - NofXd1;
+        const float NegNofXd2 = 1.0f - NofXd2;
+        o[BS_PUT] = (FutureValueX * NegNofXd2) - (s * NegNofXd1);
+    }
+}
+
+/* my_logf (bs_kernel.hpp:33-49): Taylor series of ln around 1, Horner form. */
+static float bs_dev_logf(float x)
+{
+    const float diff = x - 1.0f;
+    float r = fmaf(diff, 0.20000000f, -0.25000000f);
+    r = fmaf(r, diff, 0.33333333f);
+    r = fmaf(r, diff, -0.50000000f);
+    r = fmaf(r, diff, 1.00000000f);
+    return r * diff;
+}
+
+/* expf_0 (bs_kernel.hpp:52-65): Taylor series of exp around 0. */
+static float bs_dev_exp0(float x)
+{
+    float r = fmaf(x, 0.0083333338f, 0.04166667f);
+    r = fmaf(r, x, 0.16666666f);
+    r = fmaf(r, x, 0.5f);
+    r = fmaf(r, x, 1.0f);
+    r = fmaf(r, x, 1.0f);
+    return r;
+}
+
+/* fast_expf (bs_kernel.hpp:69-91), x < 0: whole steps of e^-1, one optional
+ * e^-0.5 step, then expf_0 of the remainder; 0 below -15. */
+static float bs_dev_fast_expf(float x)
+{
+    if (x < -15.0f) return 0.0f;
+    float part1 = 1.0f;
+    while (x <= -1.0f) {
+        part1 *= 0.36787945f;
+        x += 1.0f;
+    }
+    if (x <= -0.5f) {
+        part1 *= 0.60653066f;
+        x += 0.5f;
+    }
+    return part1 * bs_dev_exp0(x);
+}
+
+/* One CNDF of dual_CNDF (bs_kernel.hpp:95-160); the two lanes there are
+ * independent and identical. */
+static float bs_dev_cndf(float x)
+{
+    const int sign = x < 0.0f;
+    const float xa = fabsf(x);
+    const float e = bs_dev_fast_expf(-0.5f * xa * xa) * 0.39894228040143270286f;
+    float k = fmaf(0.2316419f, xa, 1.0f);
+    k = 1.0f / k;
+    float f = fmaf(k, 1.330274429f, -1.821255978f);
+    f = fmaf(f, k, 1.781477937f);
+    f = fmaf(f, k, -0.356563782f);
+    f = fmaf(f, k, 0.319381530f);
+    f = f * k;
+    float out = fmaf(-f, e, 1.0f); /* fnmsub: -(f * e) + 1, one rounding */
+    if (sign) out = 1.0f - out;
+    return out;
+}
+
+/* BlkSchlsEqEuroNoDiv_kernel restated (bs_kernel.hpp:163-198), n records in place. */
+void oracle_bs_device(float* data, long n)
+{
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        float* o = data + i * BS_REC;
+        const float s = o[BS_S], k = o[BS_STRIKE], v = o[BS_V], t = o[BS_T], r = o[BS_R];
+        const float sqrt_t = sqrtf(t);
+        const float logValues = (s == k) ? 0.0f : bs_dev_logf(s / k);
+        float xD1 = fmaf(v * v, 0.5f, r);
+        xD1 = fmaf(xD1, t, logValues);
+        const float xDen = v * sqrt_t;
+        xD1 = xD1 / xDen;
+        const float xD2 = xD1 - xDen;
+        const float c1 = bs_dev_cndf(xD1);
+        const float c2 = bs_dev_cndf(xD2);
+        const float fv = k * bs_dev_exp0(-r * t);
+        o[BS_CALL] = (s * c1) - (fv * c2);
+        const float n1 = 1.0f - c1;
+        const float n2 = 1.0f - c2;
+        o[BS_PUT] = (fv * n2) - (s * n1);
+    }
 }
 
 int oracle_version(void) { return 1; }

@@ -11,8 +11,12 @@ Function map (reference lines each one follows are in oracle.c):
   gemm_f64                        FP64 product (error measurement)
   split_bf16                      FP32 -> BF16 hi/mid/lo split
   host_jacobi                     apps/jacobi/main.cpp:19-48
+  bs_host                         apps/blackscholes/bs.hpp:5-125
+  bs_device                       apps/blackscholes/bs_kernel.hpp:33-198
+  bs_validation_error             apps/blackscholes/main.cpp:119-141
   ref_host_mm                     the reference's host_mm itself (oracle/_ref)
   ref_host_jacobi                 the reference's host_jacobi itself (oracle/_ref)
+  ref_bs_host                     the reference's BlkSchlsEqEuroNoDiv itself (oracle/_ref)
 """
 from __future__ import annotations
 
@@ -73,6 +77,10 @@ def lib():
         l.oracle_host_jacobi.restype = None
         l.oracle_fill_jacobi.argtypes = [_f32p, _L]
         l.oracle_fill_jacobi.restype = None
+        l.oracle_bs_host.argtypes = [_f32p, _L]
+        l.oracle_bs_host.restype = None
+        l.oracle_bs_device.argtypes = [_f32p, _L]
+        l.oracle_bs_device.restype = None
         _lib = l
     return _lib
 
@@ -87,6 +95,23 @@ def ref_available() -> bool:
 
 def ref_jacobi_available() -> bool:
     return os.path.exists(_REF_JACOBI_PATH)
+
+
+_REF_BS_PATH = os.path.join(_HERE, "_ref", "libref_bs.so")
+_ref_bs = None
+
+
+def ref_bs_available() -> bool:
+    return os.path.exists(_REF_BS_PATH)
+
+
+def ref_bs_lib():
+    global _ref_bs
+    if _ref_bs is None:
+        if not os.path.exists(_REF_BS_PATH):
+            raise FileNotFoundError("reference Black-Scholes host library not built (oracle/_ref)")
+        _ref_bs = ctypes.CDLL(_REF_BS_PATH)
+    return _ref_bs
 
 
 def ref_jacobi_lib():
@@ -237,6 +262,54 @@ def ref_host_jacobi(A0: np.ndarray, nx: int, ny: int, nz: int, c0: int = 2,
     out = np.zeros_like(a)
     fn(c0, c1, a, out, nx, ny, nz)
     return out
+
+
+def _bs_records(records: np.ndarray) -> np.ndarray:
+    r = np.array(records, dtype=np.float32, copy=True, order="C")
+    assert r.ndim == 2 and r.shape[1] == 8, "option records are (n, 8) float32"
+    return r
+
+
+def bs_host(records: np.ndarray) -> np.ndarray:
+    """The testbench's host reference (BlkSchlsEqEuroNoDiv, bs.hpp) on (n, 8)
+    option records; returns a copy with call and put (columns 5, 6) set."""
+    r = _bs_records(records)
+    lib().oracle_bs_host(r.ravel(), r.shape[0])
+    return r
+
+
+def bs_device(records: np.ndarray) -> np.ndarray:
+    """The device kernel's arithmetic (BlkSchlsEqEuroNoDiv_kernel,
+    bs_kernel.hpp) on (n, 8) option records; returns a copy with call and put
+    set."""
+    r = _bs_records(records)
+    lib().oracle_bs_device(r.ravel(), r.shape[0])
+    return r
+
+
+def ref_bs_host(records: np.ndarray) -> np.ndarray:
+    """Run the reference's own BlkSchlsEqEuroNoDiv (bs.hpp, oracle/_ref)."""
+    fn = getattr(ref_bs_lib(), "hbref_bs_host")
+    fn.argtypes = [_f32p, _L]
+    fn.restype = None
+    r = _bs_records(records)
+    fn(r.ravel(), r.shape[0])
+    return r
+
+
+def bs_validation_error(actual: np.ndarray, expected: np.ndarray) -> float:
+    """The testbench's check (main.cpp:119-141): the float sum over options of
+    the squared call and put differences, accumulated in option order; the
+    testbench fails when it exceeds 0.01."""
+    a = np.asarray(actual, np.float32)
+    e = np.asarray(expected, np.float32)
+    err = np.float32(0.0)
+    dc = (a[:, 5] - e[:, 5]).astype(np.float32)
+    dp = (a[:, 6] - e[:, 6]).astype(np.float32)
+    for c, p in zip((dc * dc).astype(np.float32), (dp * dp).astype(np.float32)):
+        err = np.float32(err + c)
+        err = np.float32(err + p)
+    return float(err)
 
 
 def error_vs_f64(C: np.ndarray, ref64: np.ndarray) -> dict:

@@ -18,8 +18,17 @@ Fixtures
                                 (apps/jacobi/tests.mk:1) on its input A0[i] = i % 13,
                                 c0 = 2, c1 = 4 (main.cpp:62-73): SHA-256 of the
                                 reference host_jacobi's output (main.cpp:19-48).
+  blackscholes_32768.json       the Black-Scholes benchmark's launch num-option_32768
+                                (apps/blackscholes/tests.mk:1) on seeded synthetic
+                                option records (hb_hammerbench_b200.blackscholes.
+                                option_records(32768, seed 3)): SHA-256 of the inputs,
+                                of the reference host BlkSchlsEqEuroNoDiv's call/put
+                                (bs.hpp:60-125) and of the oracle's restatement of the
+                                device kernel's arithmetic (bs_kernel.hpp:163-198),
+                                with the testbench's error between the two
+                                (main.cpp:119-141).
 
-    python tests/golden/make_golden.py [--jacobi]   (--jacobi: only that fixture)
+    python tests/golden/make_golden.py [--jacobi | --blackscholes]   (only that fixture)
 """
 import hashlib
 import json
@@ -58,10 +67,40 @@ def jacobi_fixture():
         }, f, indent=1)
 
 
+def blackscholes_fixture():
+    from hb_hammerbench_b200.blackscholes import option_records
+    assert oracle.ref_bs_available(), "reference Black-Scholes host library not built"
+    n, seed = 32768, 3
+    rec = option_records(n, seed)
+    host = oracle.ref_bs_host(rec)
+    assert np.array_equal(host, oracle.bs_host(rec))
+    dev = oracle.bs_device(rec)
+    rng = np.random.Generator(np.random.PCG64(13))
+    idx = np.sort(rng.choice(n, 32, replace=False))
+    with open(os.path.join(HERE, "blackscholes_32768.json"), "w") as f:
+        json.dump({
+            "source": "reference BlkSchlsEqEuroNoDiv (apps/blackscholes/bs.hpp:60-125) compiled "
+                      "from the reference tree; device arithmetic: oracle_bs_device "
+                      "(bs_kernel.hpp:163-198 restated)",
+            "inputs": "option_records(32768, seed=3): (n, 8) float32 records s, strike, r, v, t, "
+                      "call, put, unused",
+            "num_option": n, "seed": seed,
+            "sha256_inputs_f32": sha(rec),
+            "sha256_host_call_put_f32": sha(host[:, 5:7]),
+            "sha256_device_call_put_f32": sha(dev[:, 5:7]),
+            "validation_error_device_vs_host": oracle.bs_validation_error(dev, host),
+            "samples": [[int(i), float(host[i, 5]), float(host[i, 6]), float(dev[i, 5]),
+                         float(dev[i, 6])] for i in idx],
+        }, f, indent=1)
+
+
 def main():
     oracle.build(REFERENCE_ROOT)
     if "--jacobi" in sys.argv:
         jacobi_fixture()
+        return
+    if "--blackscholes" in sys.argv:
+        blackscholes_fixture()
         return
     assert oracle.ref_available(), "reference host_mm not built"
 
@@ -109,6 +148,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"sgemm_uniform_N{n}_NITER{niter}.npz"),
                             A=A, B=B, C_ref=C, seed=np.int64(42))
     jacobi_fixture()
+    blackscholes_fixture()
     print("golden fixtures written to", HERE)
 
 

@@ -69,6 +69,17 @@ def test_argument_errors_before_any_launch(L):
     # leading dimensions smaller than the row length
     assert lib.hbsg_gemm(0, 0, 4, 8, 16, fake, 8, fake, 8, fake, 8, 0, None, 0, None) == L.ERR_INVALID_ARG
     assert lib.hbsg_gemm(0, 0, 4, 8, 16, fake, 16, fake, 4, fake, 8, 0, None, 0, None) == L.ERR_INVALID_ARG
+    # Black-Scholes: negative counts, null records, overlapping outputs
+    assert lib.hbsg_blackscholes(fake, -1, None) == L.ERR_INVALID_ARG
+    assert lib.hbsg_blackscholes(None, 4, None) == L.ERR_INVALID_ARG
+    assert lib.hbsg_blackscholes(None, 0, None) == L.OK
+    ins = [P(0x10000 + 0x1000 * i) for i in range(5)]
+    assert lib.hbsg_blackscholes_arrays(*ins, P(0x20000), P(0x20000 + 16), 8, None) == \
+        L.ERR_INVALID_ARG
+    assert lib.hbsg_blackscholes_arrays(*ins, ins[2], P(0x30000), 8, None) == L.ERR_INVALID_ARG
+    assert lib.hbsg_blackscholes_arrays(*ins, None, P(0x30000), 8, None) == L.ERR_INVALID_ARG
+    assert lib.hbsg_blackscholes_arrays(*ins, P(0x20000), P(0x30000), -2, None) == \
+        L.ERR_INVALID_ARG
 
 
 def test_no_device_is_reported_not_crashed(L):
@@ -77,6 +88,7 @@ def test_no_device_is_reported_not_crashed(L):
         pytest.skip("a GPU is present")
     fake = ctypes.c_void_p(0x10000)
     assert L.lib().hbsg_sgemm(fake, fake, fake, 16, 1, None) == L.ERR_NO_DEVICE
+    assert L.lib().hbsg_blackscholes(fake, 4, None) == L.ERR_NO_DEVICE
 
 
 def test_tile_table(L):

@@ -18,6 +18,13 @@ def test_general_and_grouped_names():
     assert g["GROUPED"] == 512 and g["SEED"] == 0
 
 
+def test_blackscholes_names():
+    # apps/blackscholes/tests.mk:1 registers num-option_32768
+    assert sweep.parse_case("num-option_32768") == {"NUM-OPTION": 32768}
+    c = sweep.parse_case("num-option_10000000__LAYOUT_arrays")
+    assert c == {"NUM-OPTION": 10000000, "LAYOUT": "arrays"}
+
+
 @pytest.mark.parametrize("bad", ["N_512__V_fp64", "NITER_2", "N__512", "SEED_1__V_ffma"])
 def test_bad_names(bad):
     with pytest.raises(ValueError):
