@@ -82,14 +82,19 @@ static SplitLayout split_layout(int M, int N, int K, int variant) {
   return L;
 }
 
-// Workspace layout of a fused-split schedule: only the scaled forms' row and
-// column maxima (the parts never reach HBM), then the K-slice partials.
-static SplitLayout fused_layout(int M, int N, int variant) {
+// Workspace layout of a fused-split schedule: the scaled forms' row and
+// column maxima and, for the A-in-TMEM tiles, B's parts from the split pass
+// (A's parts never reach HBM; the CTA-pair tiles split B in the kernel too);
+// the K-slice partials follow.
+static SplitLayout fused_layout(int M, int N, int K, int variant, bool ts) {
   SplitLayout L{};
+  L.Kp = (K + 31) / 32 * 32;
+  if (L.Kp == 0) L.Kp = 32;
   L.rowmax_off = 0;
   L.colmax_off = scaled_of(variant) ? align256((size_t)M * 4) : 0;
-  L.total = L.colmax_off + (scaled_of(variant) ? align256((size_t)N * 4) : 0);
-  L.a_off = L.b_off = L.total;
+  L.b_off = L.colmax_off + (scaled_of(variant) ? align256((size_t)N * 4) : 0);
+  L.total = L.b_off + (ts ? align256((size_t)parts_of(variant) * N * L.Kp * 2) : 0);
+  L.a_off = L.total;
   return L;
 }
 
@@ -131,20 +136,25 @@ static void tc_pick_auto(int M, int N, int K, int variant, int sms, int req, boo
   const double t_unfused = t_split + flops / (kRate * score) + maxima;
   double best = 0.0;
   int best_idx = -1;
-  const int pairs = sms / 2;
   for (int f = 0; f < fused_num_tiles(); ++f) {
     if (fused_tile_parts(f) != P) continue;
     const int bn = fused_tile_bn(f);
-    const long tiles = (long)((M + 255) / 256) * ((N + bn - 1) / bn);
+    const int bm = fused_tile_bm(f);
+    const int slots = fused_tile_slots(f, sms);
+    const long tiles = (long)((M + bm - 1) / bm) * ((N + bn - 1) / bn);
     int kts = 0;
     const int s = fused_pick_splits(f, M, N, K, req, sms, &kts);
-    const long waves = (tiles * s + pairs - 1) / pairs;
+    const long waves = (tiles * s + slots - 1) / slots;
     const double t_conv = (double)waves * kts * fused_ktile_cycles(f) / kClock;
     const double t_mem = opnds * 4.0 / kHbm;
     const double t_reduce = s > 1 ? (double)s * M * N * 8.0 / kHbm : 0.0;
     // + ~3 us per wave to fill and drain the pipeline (first staging loads,
     // last MMAs, epilogue stores)
-    const double t = (t_conv > t_mem ? t_conv : t_mem) + 3e-6 * waves + t_reduce + maxima;
+    // A-in-TMEM tiles split B in a pass of their own first
+    const double t_split_b =
+        fused_tile_ts(f) ? (double)K * N * (4.0 + 2.0 * P) / (0.9 * kHbm) + 4e-6 : 0.0;
+    const double t = (t_conv > t_mem ? t_conv : t_mem) + 3e-6 * waves + t_reduce + maxima +
+                     t_split_b;
     if (best_idx < 0 || t < best) {
       best = t;
       best_idx = f;
@@ -206,7 +216,8 @@ static size_t workspace_needed(int M, int N, int K, int batch, int variant, cons
   TcChoice ch;
   if (!tc_schedule(M, N, K, variant, cfg, sms, transposed, fusable == 1, &ch)) return 0;
   const size_t partial = ch.splits > 1 ? align256((size_t)ch.splits * M * N * 4) : 0;
-  return (ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant)).total + partial;
+  return (ch.fused ? fused_layout(M, N, K, variant, fused_tile_ts(ch.idx))
+                   : split_layout(M, N, K, variant)).total + partial;
 }
 
 // Whether gemm_dispatch may run these operands on a fused-split tile.
@@ -284,7 +295,8 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   if (!tc_schedule(M, N, K, variant, cfg, sms, trans_a || trans_b, fusable, &ch))
     return HBSG_ERR_UNSUPPORTED;
   const int tc = ch.idx, splits = ch.splits;
-  const SplitLayout L = ch.fused ? fused_layout(M, N, variant) : split_layout(M, N, K, variant);
+  const SplitLayout L = ch.fused ? fused_layout(M, N, K, variant, fused_tile_ts(tc))
+                                 : split_layout(M, N, K, variant);
   const size_t partial_bytes = splits > 1 ? align256((size_t)splits * M * N * 4) : 0;
   if (L.total + partial_bytes > 0 &&
       (!ws || ws_bytes < L.total + partial_bytes || (reinterpret_cast<uintptr_t>(ws) & 255)))
@@ -298,15 +310,21 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
   const int raster = cfg && cfg->raster_group > 0 ? cfg->raster_group : 0;
   const int chunk = cfg && cfg->chunk_k > 0 ? cfg->chunk_k : 0;
   if (ch.fused) {
-    // The split runs inside the product kernel; the workspace holds only the
-    // scaled forms' maxima (PRESPLIT_A / _B: already current) and partials.
+    // The split of A (and, on the CTA-pair tiles, of B) runs inside the
+    // product kernel; the workspace holds the scaled forms' maxima, the
+    // A-in-TMEM tiles' B parts (PRESPLIT_A / _B: already current) and partials.
+    const bool ts = fused_tile_ts(tc) != 0;
     for (int b = 0; b < batch; ++b) {
       const float* Ab = A + b * strideA;
       const float* Bb = B + b * strideB;
       cudaError_t e = cudaSuccess;
       if (scaled && !(flags & HBSG_FLAG_PRESPLIT_A)) e = maxabs_rows(Ab, lda, M, K, rowmax, st);
-      if (e == cudaSuccess && scaled && !(flags & HBSG_FLAG_PRESPLIT_B))
-        e = maxabs_cols(Bb, ldb, K, N, colmax, st);
+      if (e == cudaSuccess && !(flags & HBSG_FLAG_PRESPLIT_B)) {
+        if (ts)  // B's parts (and the scaled forms' column maxima)
+          e = split_operand_b(Bb, ldb, K, N, L.Kp, P, scaled, Bp, colmax, sms, st);
+        else if (scaled)
+          e = maxabs_cols(Bb, ldb, K, N, colmax, st);
+      }
       if (e != cudaSuccess) return status_from(e);
       if (flags & HBSG_FLAG_SPLIT_ONLY) continue;
       FusedParams fp{};
@@ -323,6 +341,8 @@ static int gemm_dispatch(int trans_a, int trans_b, int M, int N, int K, const fl
       fp.kt_per_split = ch.kts;
       fp.rowmax = rowmax;
       fp.colmax = colmax;
+      fp.Bparts = ts ? Bp : nullptr;
+      fp.Kp = L.Kp;
       e = fused_launch(tc, fp, raster, chunk, sms, 0, st,
                        reinterpret_cast<float*>(w + L.total));
       if (e != cudaSuccess) return status_from(e);

@@ -659,7 +659,9 @@ static bool tile_shape(int variant, const hbsg_config* cfg, int* ffma_idx, int* 
   int idx = -1;
   if (tile >= nf + tc_num_tiles()) {  // a fused-split tile
     const int f = tile - nf - tc_num_tiles();
-    if (f >= fused_num_tiles() || fused_tile_parts(f) != P) return false;
+    // grouped plans run the CTA-pair fused tiles only (the first entries of
+    // the fused table)
+    if (f >= fused_num_tiles() || fused_tile_ts(f) || fused_tile_parts(f) != P) return false;
     fused_tile_info(f, &info);
     *ffma_idx = -1;
     *tc_idx = -1;

@@ -76,11 +76,18 @@ struct FusedParams {
   int kt_per_split;  // k-tiles (of 32) per slice
   const uint32_t* rowmax;  // scaled forms: FP32 bit patterns of max|A row| / max|B column|
   const uint32_t* colmax;
+  // A-in-TMEM tiles (fused_tile_ts): B's BF16 parts made by the split pass,
+  // parts[P][N][Kp] (the unfused kernels' layout); unused by the pair tiles
+  const void* Bparts;
+  int Kp;
 };
 int fused_num_tiles();
 bool fused_tile_info(int idx, hbsg_tile_info* out);
 int fused_tile_parts(int idx);
 int fused_tile_bn(int idx);
+int fused_tile_bm(int idx);     // output rows per tile (256: CTA pair, 128: A in TMEM)
+int fused_tile_ts(int idx);     // 1: the A-in-TMEM single-CTA form
+int fused_tile_slots(int idx, int sms);  // concurrent work units (clusters or CTAs)
 int fused_pick_splits(int idx, int M, int N, int K, int requested, int sms, int* kt_per_split);
 // C = A*B on fused entry idx; partial: [splits][M][N] FP32 when p.splits > 1.
 cudaError_t fused_launch(int idx, FusedParams p, int raster, int chunk_k, int sms,

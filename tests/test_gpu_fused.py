@@ -27,7 +27,7 @@ def fused_ids(hb):
     for t in hb.tiles():
         if t["family"] != "bf16":
             continue
-        if t["fused"]:
+        if t["fused"] and t["bm"] == 256:  # CTA-pair tiles (the A-in-TMEM ones: test_gpu_fused_ts.py)
             fused[(t["parts"], t["bn"])] = t["tile"]
         elif t["bm"] == 128:
             plain[(t["parts"], t["bn"])] = t["tile"]

@@ -1,0 +1,168 @@
+"""Fused-split tiles that keep A's BF16 parts in tensor memory (single CTA,
+128 x 64 output tiles, tcgen05.mma with A from TMEM) on the GPU, through the
+C ABI.
+
+The A converters write the same split values into tensor memory that the
+split pass writes to HBM, the B converters write B's parts in the unfused
+operand layout, and products, product order and TMEM drains are those of the
+unfused kernels, so each result is bit-identical to the unfused single-CTA
+tile of the same product count and width. Bars otherwise as in
+test_gpu_bf16.py.
+"""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PARTS = {"bf16x6": 3, "bf16x3": 2, "bf16x6_scaled": 3, "bf16x3_scaled": 2}
+
+
+@pytest.fixture(scope="module")
+def hb():
+    import hb_hammerbench_b200 as hb
+    return hb
+
+
+@pytest.fixture(scope="module")
+def ids(hb):
+    """({parts: A-in-TMEM tile id}, {parts: unfused single-CTA BN = 64 tile id})."""
+    ts, plain = {}, {}
+    for t in hb.tiles():
+        if t["family"] != "bf16" or t["bn"] != 64:
+            continue
+        if t["fused"] and t["bm"] == 128:
+            ts[t["parts"]] = t["tile"]
+        elif not t["fused"] and t["bm"] == 128:
+            plain[t["parts"]] = t["tile"]
+    assert set(ts) == {2, 3} and set(plain) == {2, 3}
+    return ts, plain
+
+
+def _rand(shape, seed, wide=False):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    rows, cols = shape
+    pad = (cols + 3) // 4 * 4
+    x = torch.rand((rows, pad), device="cuda", generator=g) * 2 - 1
+    if wide:
+        u = torch.rand((rows, pad), device="cuda", generator=g) * 40 - 20
+        x = torch.sign(x) * torch.exp2(u)
+    return x[:, :cols]
+
+
+def _err(C, ref):
+    import torch
+    d = C.double() - ref
+    return float(torch.linalg.norm(d) / torch.linalg.norm(ref))
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3", "bf16x6_scaled", "bf16x3_scaled"])
+@pytest.mark.parametrize("m,n,k", [(128, 64, 32), (256, 64, 64), (300, 200, 100),
+                                   (1000, 700, 1031), (64, 520, 7), (777, 64, 2048),
+                                   (4099, 33, 4100)])
+def test_ts_matches_unfused(hb, ids, variant, m, n, k):
+    import torch
+    ts, plain = ids
+    P = PARTS[variant]
+    wide = "scaled" in variant
+    A = _rand((m, k), m + 3 * k, wide)
+    B = _rand((k, n), n + 7 * k, wide)
+    cfg = {"split_k": 1, "chunk_k": 64}
+    Ct = hb.gemm(A, B, variant=variant, config={**cfg, "tile": ts[P]})
+    Cu = hb.gemm(A, B, variant=variant, config={**cfg, "tile": plain[P]})
+    assert torch.equal(Ct, Cu)
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
+@pytest.mark.parametrize("chunk_k", [32, 256])
+def test_ts_drain_intervals(hb, ids, variant, chunk_k):
+    import torch
+    ts, plain = ids
+    P = PARTS[variant]
+    A = _rand((512, 3000), 41)
+    B = _rand((3000, 64), 42)
+    cfg = {"split_k": 1, "chunk_k": chunk_k}
+    assert torch.equal(hb.gemm(A, B, variant=variant, config={**cfg, "tile": ts[P]}),
+                       hb.gemm(A, B, variant=variant, config={**cfg, "tile": plain[P]}))
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
+@pytest.mark.parametrize("m,n,k,splits", [(256, 64, 65536, 0), (300, 50, 4096, 3),
+                                           (512, 64, 20000, 0)])
+def test_ts_split_k(hb, ids, variant, m, n, k, splits):
+    import torch
+    ts, plain = ids
+    P = PARTS[variant]
+    A = _rand((m, k), k + 11)
+    B = _rand((k, n), k + 12)
+    ref = A.double() @ B.double()
+    cfg = {"split_k": splits, "tile": ts[P]}
+    C1 = hb.gemm(A, B, variant=variant, config=cfg)
+    C2 = hb.gemm(A, B, variant=variant, config=cfg)
+    assert torch.equal(C1, C2)  # fixed reduction order
+    e = _err(C1, ref)
+    if P == 3:
+        assert e <= _err(hb.gemm(A, B), ref), e  # no worse than FFMA
+    else:
+        assert e <= 2.0 ** -16
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3_scaled"])
+def test_ts_zero_k_gives_zeros(hb, ids, variant):
+    import torch
+    ts, _ = ids
+    A = torch.empty((300, 0), device="cuda")
+    B = torch.empty((0, 200), device="cuda")
+    C = torch.full((300, 200), 7.0, device="cuda")
+    hb.gemm(A, B, C, variant=variant, config={"tile": ts[PARTS[variant]]})
+    assert torch.count_nonzero(C).item() == 0
+
+
+def test_ts_reference_fixture_exact(hb, ids, oracle_mod, golden_dir):
+    import hashlib
+    import json
+    import os
+
+    import numpy as np
+    import torch
+    ts, _ = ids
+    fix = json.load(open(os.path.join(golden_dir, "sgemm_mod_N512_NITER2.json")))
+    n, niter = fix["N"], fix["NITER"]
+    m1, m2 = oracle_mod.fill_mod(niter * n * n)
+    a = torch.from_numpy(m1).cuda().view(niter, n, n)
+    b = torch.from_numpy(m2).cuda().view(niter, n, n)
+    out = torch.empty_like(a)
+    for i in range(niter):
+        hb.gemm(a[i], b[i], out[i], variant="bf16x6", config={"tile": ts[3]})
+    got = out.cpu().numpy()
+    assert hashlib.sha256(np.ascontiguousarray(got).tobytes()).hexdigest() == fix["sha256_result_f32"]
+
+
+def test_ts_rejected_where_unsupported(hb, ids):
+    ts, _ = ids
+    A = _rand((64, 96), 1)
+    B = _rand((96, 64), 2)
+    with pytest.raises(hb.HbsgError) as e:  # transposed operands
+        hb.gemm(A.t().contiguous(), B, variant="bf16x6", trans_a=True, config={"tile": ts[3]})
+    assert e.value.status == -2
+    with pytest.raises(hb.HbsgError):  # grouped plans run the CTA-pair fused tiles only
+        hb.GroupedPlan([A], [B], variant="bf16x6", config={"tile": ts[3]})
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
+def test_ts_tall_m_config(hb, ids, variant):
+    """65536 x 64 x 4096 (the tall, narrow benchmark shape): bit-identical to
+    the unfused tile, X6 no worse than FFMA against FP64."""
+    import torch
+    ts, plain = ids
+    P = PARTS[variant]
+    A = _rand((65536, 4096), 5)
+    B = _rand((4096, 64), 6)
+    Ct = hb.gemm(A, B, variant=variant, config={"tile": ts[P], "split_k": 1})
+    Cu = hb.gemm(A, B, variant=variant, config={"tile": plain[P], "split_k": 1})
+    assert torch.equal(Ct, Cu)
+    ref = A.double() @ B.double()
+    e = _err(Ct, ref)
+    if P == 3:
+        assert e <= _err(hb.gemm(A, B, variant="ffma"), ref)
+    else:
+        assert e <= 2.0 ** -16
