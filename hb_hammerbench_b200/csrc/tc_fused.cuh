@@ -27,7 +27,8 @@
 // bandwidth, has no room for.
 //
 // CTA (512 threads, 16 warps, one CTA per SM, clusters of two):
-//   warp 0       TMEM allocation; lane 0 of the leader CTA issues the MMAs
+//   warp 0       TMEM allocation; the leader CTA's warp issues the MMAs
+//                (one elected lane)
 //   warp 1       lane 0: TMA loads of the FP32 staging ring
 //   warps 2-7    converters (this CTA's 128 A rows and BN/2 B columns)
 //   warps 8-15   epilogue (TMEM lane quadrant warp % 4, column half)
@@ -372,7 +373,9 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
   if (warp < 8) regs_dec<kRegsLow>();
   if (warp == 0) {
     // ---------------- MMA issuer (leader CTA only) ----------------
-    if (leader && lane == 0) {
+    // The whole warp runs the loop converged and one elected lane issues
+    // (tc_mma_elect); a wait passes only when it passed on every lane.
+    if (leader) {
       // full-width MMAs: each CTA holds a fixed half of the BN columns, so the
       // instruction's N cannot be trimmed (padding columns are zeros)
       constexpr uint32_t idesc = f16_idesc(2 * kBM, BN);
@@ -385,7 +388,8 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
         int kt = 0;
         for (int c = 0; c < nchunks && ok; ++c, ++ch) {
           const int buf = ch & 1;
-          if (!wait_bounded(&tempty[buf], ((ch >> 1) & 1) ^ 1, abort_flag, lim)) {
+          if (!__all_sync(0xffffffffu,
+                          wait_bounded(&tempty[buf], ((ch >> 1) & 1) ^ 1, abort_flag, lim))) {
             ok = false;
             break;
           }
@@ -395,7 +399,8 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
           bool first = true;
           for (; kt < kend; ++kt, ++it) {
             const int s = it % STAGES;
-            if (!wait_bounded_cluster(&full[s], (it / STAGES) & 1, abort_flag, lim)) {
+            if (!__all_sync(0xffffffffu, wait_bounded_cluster(&full[s], (it / STAGES) & 1,
+                                                              abort_flag, lim))) {
               ok = false;
               break;
             }
@@ -408,13 +413,13 @@ __device__ __forceinline__ void tc_fused_body(const Tiles& tiles, const TcRun& r
               for (int q = 0; q < Products<P>::n; ++q) {
                 const uint64_t ad = sw64_desc(sa + Products<P>::a(q) * S::kABytes + ks * 32);
                 const uint64_t bd = sw64_desc(sb + Products<P>::b(q) * S::kBBytes + ks * 32);
-                tc_mma_pair(d, ad, bd, idesc, first ? 0u : 1u);
+                tc_mma_pair_elect(d, ad, bd, idesc, first ? 0u : 1u);
                 first = false;
               }
             }
-            tc_commit_pair(&empty[s]);
+            tc_commit_pair_elect(&empty[s]);
           }
-          if (ok) tc_commit_pair(&tfull[buf]);
+          if (ok) tc_commit_pair_elect(&tfull[buf]);
         }
       }
     }

@@ -110,19 +110,6 @@ HBSG_DEV void tc_mma_ts_elect(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, 
       "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// tcgen05.commit to an mbarrier from one elected lane of a converged warp.
-HBSG_DEV void tc_commit_elect(uint64_t* bar) {
-  asm volatile(
-      "{\n\t.reg .pred e;\n\t.reg .b32 l;\n\t"
-      "elect.sync l|e, 0xffffffff;\n\t"
-      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-
-// Tiles::get gives, for a work item, the FP32 A map (w.ma, box {32, 128},
-// 128-byte swizzle) and the B parts map (w.mb, box {32, BN, P}).
 template <int P, int BN, int SA, int SB, int TSTAGES, bool SCALED, class Tiles>
 __device__ __forceinline__ void tc_fused_ts_body(const Tiles& tiles, const TcRun& run) {
   using S = TcTsShape<P, BN, SA, SB, TSTAGES>;

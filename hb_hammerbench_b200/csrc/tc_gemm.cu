@@ -13,7 +13,8 @@
 //   warp 0      TMA producer: per k-tile one 3-D box of all A parts and one
 //               of all B parts into a STAGES-deep shared-memory ring
 //               (64-byte swizzle, K-major), completion on an mbarrier.
-//   warp 1      TMEM allocator and MMA issuer: one thread issues
+//   warp 1      TMEM allocator and MMA issuer: the warp runs the issue loop
+//               converged and one elected lane issues
 //               tcgen05.mma kind::f16 (M=128, N=BN, K=16) per product and
 //               k-step into TMEM buffer (chunk % 2); tcgen05.commit frees the
 //               smem stage and, at the end of a chunk, hands the buffer to

@@ -58,22 +58,26 @@ HBSG_DEV void tma_load_3d_pair(uint32_t dst, const CUtensorMap* map, int c0, int
       : "memory");
 }
 
-HBSG_DEV void tc_mma_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                          uint32_t accumulate) {
+// The pair MMA, and the commit that arrives (once) on the barrier at this
+// offset in both CTAs of the pair when all prior tensor-core work of the
+// issuing thread completes; from one elected lane of a converged warp (see
+// tc_mma_elect).
+HBSG_DEV void tc_mma_pair_elect(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                uint32_t accumulate) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\t"
+      "{\n\t.reg .pred p, e;\n\t.reg .b32 l;\n\t"
+      "elect.sync l|e, 0xffffffff;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "@e tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// Arrive (once) on the barrier at this offset in both CTAs of the pair when
-// all prior tensor-core work of this thread completes.
-HBSG_DEV void tc_commit_pair(uint64_t* bar) {
+HBSG_DEV void tc_commit_pair_elect(uint64_t* bar) {
   asm volatile(
-      "{\n\t.reg .b16 m;\n\t"
+      "{\n\t.reg .b16 m;\n\t.reg .pred e;\n\t.reg .b32 l;\n\t"
+      "elect.sync l|e, 0xffffffff;\n\t"
       "mov.b16 m, 3;\n\t"
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      "@e tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
       " [%0], m;\n\t}\n" ::"r"(smem_u32(bar))
       : "memory");
 }
@@ -169,7 +173,9 @@ __device__ __forceinline__ void tc_pair_body(const Tiles& tiles, const TcRun& ru
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer (leader CTA only) ----------------
-    if (leader && lane == 0) {
+    // The whole warp runs the loop converged and one elected lane issues
+    // (tc_mma_elect); a wait passes only when it passed on every lane.
+    if (leader) {
       constexpr uint32_t idesc = f16_idesc(2 * kBM, BN);
       uint32_t it = 0, ch = 0;
       bool ok = true;
@@ -179,7 +185,8 @@ __device__ __forceinline__ void tc_pair_body(const Tiles& tiles, const TcRun& ru
         int kt = 0;
         for (int c = 0; c < nchunks && ok; ++c, ++ch) {
           const int buf = ch & 1;
-          if (!wait_bounded(&tempty[buf], ((ch >> 1) & 1) ^ 1, abort_flag, lim)) {
+          if (!__all_sync(0xffffffffu,
+                          wait_bounded(&tempty[buf], ((ch >> 1) & 1) ^ 1, abort_flag, lim))) {
             ok = false;
             break;
           }
@@ -189,7 +196,8 @@ __device__ __forceinline__ void tc_pair_body(const Tiles& tiles, const TcRun& ru
           bool first = true;
           for (; kt < kend; ++kt, ++it) {
             const int s = it % STAGES;
-            if (!wait_bounded(&full[s], (it / STAGES) & 1, abort_flag, lim)) {
+            if (!__all_sync(0xffffffffu,
+                            wait_bounded(&full[s], (it / STAGES) & 1, abort_flag, lim))) {
               ok = false;
               break;
             }
@@ -202,13 +210,13 @@ __device__ __forceinline__ void tc_pair_body(const Tiles& tiles, const TcRun& ru
               for (int q = 0; q < Products<P>::n; ++q) {
                 const uint64_t ad = sw64_desc(sa + Products<P>::a(q) * S::kABytes + ks * 32);
                 const uint64_t bd = sw64_desc(sb + Products<P>::b(q) * S::kBBytes + ks * 32);
-                tc_mma_pair(d, ad, bd, idesc, first ? 0u : 1u);
+                tc_mma_pair_elect(d, ad, bd, idesc, first ? 0u : 1u);
                 first = false;
               }
             }
-            tc_commit_pair(&empty[s]);
+            tc_commit_pair_elect(&empty[s]);
           }
-          if (ok) tc_commit_pair(&tfull[buf]);
+          if (ok) tc_commit_pair_elect(&tfull[buf]);
         }
       }
     }
