@@ -166,3 +166,32 @@ def test_ts_tall_m_config(hb, ids, variant):
         assert e <= _err(hb.gemm(A, B, variant="ffma"), ref)
     else:
         assert e <= 2.0 ** -16
+
+
+def test_ts_workspace_holds_b_parts(hb, ids):
+    """The A-in-TMEM tiles keep B's parts in the workspace (P x N x K padded to
+    32, bf16); a workspace 256 bytes short is rejected through the C ABI
+    (status -3) before any launch, and the full one gives the same result as
+    the host interface's own allocation."""
+    import ctypes
+
+    import torch
+    from hb_hammerbench_b200 import _lib
+    ts, _ = ids
+    m, n, k = 4096, 64, 4100
+    for v, P in (("bf16x6", 3), ("bf16x3", 2)):
+        cfg = {"tile": ts[P], "split_k": 1}
+        need = hb.gemm_workspace_size(m, n, k, v, cfg)
+        assert need >= P * n * ((k + 31) // 32 * 32) * 2
+        A = _rand((m, k), 7)
+        B = _rand((k, n), 8)
+        C = torch.empty((m, n), device="cuda")
+        ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+        c = ctypes.pointer(_lib.Config(**cfg))
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        args = (0, 0, m, n, k, ctypes.c_void_p(A.data_ptr()), A.stride(0),
+                ctypes.c_void_p(B.data_ptr()), B.stride(0), ctypes.c_void_p(C.data_ptr()),
+                C.stride(0), _lib.VARIANTS[v], c, ctypes.c_void_p(ws.data_ptr()))
+        assert _lib.lib().hbsg_gemm_ex(*args, need - 256, stream) == _lib.ERR_WORKSPACE
+        assert _lib.lib().hbsg_gemm_ex(*args, need, stream) == _lib.OK
+        assert torch.equal(C, hb.gemm(A, B, variant=v, config=cfg))
