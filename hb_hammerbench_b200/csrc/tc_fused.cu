@@ -138,6 +138,10 @@ static cudaError_t launch_fused_ts(const CUtensorMap& a, const CUtensorMap& b,
   const void* k = fused_ts_kernel_ptr<P, BN, SA, SB, TSTAGES>(scaled);
   static uint64_t masks[2] = {0, 0};
   if (!set_smem_once(k, S::kSmemBytes, &masks[scaled ? 1 : 0])) return cudaErrorInvalidValue;
+  if (BN > 64) {  // the body's setmaxnreg split needs exactly 128 registers at launch
+    static int regs_ok[2] = {0, 0};
+    if (!fused_regs_ok(k, &regs_ok[scaled ? 1 : 0])) return cudaErrorInvalidConfiguration;
+  }
   if (scaled)
     tc_fused_ts_kernel<P, BN, SA, SB, TSTAGES, true><<<grid, kTsThreads, S::kSmemBytes, st>>>(a, b, p, run);
   else

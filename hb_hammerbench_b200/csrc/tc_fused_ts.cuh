@@ -1,6 +1,6 @@
 // Fused-split tensor-core GEMM body with the A operand's BF16 parts in tensor
 // memory (tcgen05.mma with A from TMEM, single CTA, sm_100a): the tile for
-// narrow outputs (N <= 64 per tile, e.g. 65536 x 64 x 4096).
+// narrow outputs (64- or 128-column tiles, e.g. 65536 x 64 x 4096).
 //
 // Why: with a narrow B tile the shared-memory traffic per MMA flop of the
 // CTA-pair fused tiles (tc_fused.cuh) is dominated by A: for 128 rows x 32 k
@@ -58,10 +58,19 @@ namespace hbsg {
 // (parts, BN, A staging stages, B parts stages, TMEM A slots)
 #define HBSG_FUSED_TS_TILE_LIST(X) \
   X(3, 64, 6, 8, 8)                \
-  X(2, 64, 8, 8, 12)
+  X(2, 64, 8, 8, 12)               \
+  X(3, 128, 4, 5, 4)               \
+  X(2, 128, 6, 6, 8)
 
 static constexpr int kTsThreads = 512;
 static constexpr int kTsAGroups = 2;  // A converter groups of 4 warps, alternating k-tiles
+// Tiles wider than 64 columns: the epilogue warpgroup holds BN FP32 sums per
+// thread, so setmaxnreg moves registers to it from the other three
+// warpgroups (3 x 128 x 112 + 128 x 176 = 65536, the block's launch
+// allotment of 512 threads x 128).
+static constexpr int kTsRegsLow = 112;
+static constexpr int kTsRegsHigh = 176;
+static_assert(3 * 128 * kTsRegsLow + 128 * kTsRegsHigh == 65536, "register split");
 
 template <int P, int BN, int SA, int SB, int TSTAGES>
 struct TcTsShape {
@@ -166,6 +175,11 @@ __device__ __forceinline__ void tc_fused_ts_body(const Tiles& tiles, const TcRun
   const uint32_t tmem_base = *tmem_slot;
   const unsigned long long lim = run.wait_limit_ns;
 
+  // each role's code sits inside the branch that set its register count
+  constexpr bool kSplitRegs = BN > 64;
+  if constexpr (kSplitRegs) {
+    if (warp < 12) regs_dec<kTsRegsLow>();
+  }
   if (warp == 0 || warp == 2) {
     // ---------------- TMA loads: A staging (warp 0), B parts (warp 2) ----------------
     // A: 128 rows x 32 k of FP32 (rows and k beyond the matrix arrive as
@@ -325,6 +339,7 @@ __device__ __forceinline__ void tc_fused_ts_body(const Tiles& tiles, const TcRun
     }
   } else if (warp >= 12) {
     // ---------------- epilogue (warps 12-15) ----------------
+    if constexpr (kSplitRegs) regs_inc<kTsRegsHigh>();
     const int q = warp & 3;
     uint32_t ch = 0;
     bool ok = true;

@@ -23,18 +23,22 @@ def hb():
 
 
 @pytest.fixture(scope="module")
-def ids(hb):
-    """({parts: A-in-TMEM tile id}, {parts: unfused single-CTA BN = 64 tile id})."""
+def all_ids(hb):
+    """({(parts, bn): A-in-TMEM tile id}, {(parts, bn): unfused single-CTA tile id})."""
     ts, plain = {}, {}
     for t in hb.tiles():
-        if t["family"] != "bf16" or t["bn"] != 64:
+        if t["family"] != "bf16" or t["bm"] != 128:
             continue
-        if t["fused"] and t["bm"] == 128:
-            ts[t["parts"]] = t["tile"]
-        elif not t["fused"] and t["bm"] == 128:
-            plain[t["parts"]] = t["tile"]
-    assert set(ts) == {2, 3} and set(plain) == {2, 3}
+        (ts if t["fused"] else plain)[(t["parts"], t["bn"])] = t["tile"]
+    assert set(ts) == {(3, 64), (2, 64), (3, 128), (2, 128)}
     return ts, plain
+
+
+@pytest.fixture(scope="module")
+def ids(all_ids):
+    """The 64-wide tiles: ({parts: A-in-TMEM id}, {parts: unfused id})."""
+    ts, plain = all_ids
+    return ({p: ts[(p, 64)] for p in (2, 3)}, {p: plain[(p, 64)] for p in (2, 3)})
 
 
 def _rand(shape, seed, wide=False):
@@ -56,20 +60,55 @@ def _err(C, ref):
 
 
 @pytest.mark.parametrize("variant", ["bf16x6", "bf16x3", "bf16x6_scaled", "bf16x3_scaled"])
+@pytest.mark.parametrize("bn", [64, 128])
 @pytest.mark.parametrize("m,n,k", [(128, 64, 32), (256, 64, 64), (300, 200, 100),
                                    (1000, 700, 1031), (64, 520, 7), (777, 64, 2048),
                                    (4099, 33, 4100)])
-def test_ts_matches_unfused(hb, ids, variant, m, n, k):
+def test_ts_matches_unfused(hb, all_ids, variant, bn, m, n, k):
     import torch
-    ts, plain = ids
+    ts, plain = all_ids
     P = PARTS[variant]
     wide = "scaled" in variant
     A = _rand((m, k), m + 3 * k, wide)
     B = _rand((k, n), n + 7 * k, wide)
     cfg = {"split_k": 1, "chunk_k": 64}
-    Ct = hb.gemm(A, B, variant=variant, config={**cfg, "tile": ts[P]})
-    Cu = hb.gemm(A, B, variant=variant, config={**cfg, "tile": plain[P]})
+    Ct = hb.gemm(A, B, variant=variant, config={**cfg, "tile": ts[(P, bn)]})
+    Cu = hb.gemm(A, B, variant=variant, config={**cfg, "tile": plain[(P, bn)]})
     assert torch.equal(Ct, Cu)
+
+
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
+def test_ts128_split_k_and_fixture(hb, all_ids, oracle_mod, golden_dir, variant):
+    """128-wide A-in-TMEM tiles: fixed-order split-K and the i % 7 / i % 3
+    fixture's SHA-256 (X6)."""
+    import hashlib
+    import json
+    import os
+
+    import numpy as np
+    import torch
+    ts, _ = all_ids
+    P = PARTS[variant]
+    A = _rand((384, 20000), 31)
+    B = _rand((20000, 200), 32)
+    cfg = {"split_k": 0, "tile": ts[(P, 128)]}
+    C1 = hb.gemm(A, B, variant=variant, config=cfg)
+    assert torch.equal(C1, hb.gemm(A, B, variant=variant, config=cfg))
+    ref = A.double() @ B.double()
+    e = _err(C1, ref)
+    assert e <= (_err(hb.gemm(A, B), ref) if P == 3 else 2.0 ** -16), e
+    if P == 3:
+        fix = json.load(open(os.path.join(golden_dir, "sgemm_mod_N512_NITER2.json")))
+        n, niter = fix["N"], fix["NITER"]
+        m1, m2 = oracle_mod.fill_mod(niter * n * n)
+        a = torch.from_numpy(m1).cuda().view(niter, n, n)
+        b = torch.from_numpy(m2).cuda().view(niter, n, n)
+        out = torch.empty_like(a)
+        for i in range(niter):
+            hb.gemm(a[i], b[i], out[i], variant="bf16x6", config={"tile": ts[(3, 128)]})
+        got = out.cpu().numpy()
+        assert hashlib.sha256(np.ascontiguousarray(got).tobytes()).hexdigest() == \
+            fix["sha256_result_f32"]
 
 
 @pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
