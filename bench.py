@@ -524,6 +524,7 @@ BS_LEGS = [
     ("blackscholes_10M_records", "num-option_10000000"),
     ("blackscholes_10M_arrays", "num-option_10000000__LAYOUT_arrays"),
 ]
+JACOBI_LEG = ("jacobi_512x512x512", "nx_512__ny_512__nz_512")
 
 
 def _config_legs(hb, peaks: dict, fp32_tflops: float, single_x6: float, single_ffma) -> dict:
@@ -572,6 +573,16 @@ def _config_legs(hb, peaks: dict, fp32_tflops: float, single_x6: float, single_f
                                  "frac": r["dram_gbs"] / peaks["hbm_gbs"],
                                  "bytes_per_option": r["bytes_per_option"]}}
         torch.cuda.empty_cache()
+    # Jacobi 7-point step (apps/jacobi) on a 512^3 grid (512 MB in, 512 MB
+    # out, larger than L2): HBM-bound at 8 bytes per point
+    key, case = JACOBI_LEG
+    r = sweep.run_case(case, steps=20, warmup=3)
+    out[key] = {"case": case, "value": r["gpoints_per_s"], "unit": "Gpoints/s",
+                "ms_per_step": r["ms"], "changed_after_repeat": r["changed_after_repeat"],
+                "roofline": {"bound": "hbm", "achieved": r["dram_gbs"], "peak": peaks["hbm_gbs"],
+                             "unit": "GB/s", "frac": r["dram_gbs"] / peaks["hbm_gbs"],
+                             "bytes_per_point": r["bytes_per_point"]}}
+    torch.cuda.empty_cache()
     return out
 
 

@@ -19,10 +19,12 @@ KEY_value fields. Recognised keys:
   num-option_<n>             Black-Scholes (apps/blackscholes/tests.mk:1): n seeded
                              synthetic option records priced in place
   LAYOUT_<l>                 Black-Scholes layout: records (default) | arrays
+  nx_<x>__ny_<y>__nz_<z>     Jacobi 7-point step (apps/jacobi/tests.mk:1-2) on a
+                             seeded U[-1,1) grid, c0 = 2, c1 = 4
 
 Examples: N_512__NITER_2, N_8192__NITER_1__V_bf16x6, M_256__N_256__K_1048576__V_bf16x6,
 GROUPED_512__SEED_0__V_bf16x6, N_8192__NITER_1__V_bf16x6_scaled__DIST_wide,
-num-option_32768, num-option_10000000__LAYOUT_arrays.
+num-option_32768, num-option_10000000__LAYOUT_arrays, nx_512__ny_512__nz_512.
 
 Each case prints one JSON line: effective TFLOP/s (sum of 2*M*N*K over the
 step time, CUDA events over the timed steps), and unless --no-error the
@@ -33,6 +35,9 @@ Nsight Compute). Black-Scholes cases print options per second and the DRAM
 bytes per second of the layout (records: the 32-byte record read and written
 back, 64 bytes per option; arrays: 20 bytes read and 8 written), and instead
 of the FP64 error the count of options that differ from the first step.
+Jacobi cases print grid points per second and DRAM bytes per second (4 bytes
+read and 4 written per point), and the count of points that differ from the
+first step.
 """
 from __future__ import annotations
 
@@ -59,7 +64,8 @@ def parse_case(name: str) -> dict:
         out[key.upper()] = int(val) if val.lstrip("-").isdigit() else val.lower()
     if "V" in out and out["V"] not in VARIANTS:
         raise ValueError(f"unknown variant {out['V']!r}")
-    if "GROUPED" not in out and "N" not in out and "NUM-OPTION" not in out:
+    if ("GROUPED" not in out and "N" not in out and "NUM-OPTION" not in out
+            and "NX" not in out):
         raise ValueError(f"case {name!r} names no problem size")
     return out
 
@@ -152,9 +158,35 @@ def run_blackscholes(name: str, steps: int = 10, warmup: int = 3, check: bool = 
     return res
 
 
+def run_jacobi(name: str, steps: int = 10, warmup: int = 3, check: bool = True,
+               device=None) -> dict:
+    from .sgemm import jacobi
+    c = parse_case(name)
+    nx, ny, nz = c["NX"], c["NY"], c["NZ"]
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=device).manual_seed(c.get("SEED", 0))
+    a = torch.rand(nx * ny * nz, device=device, generator=g) * 2 - 1
+    out = torch.empty_like(a)
+
+    def step():
+        jacobi(a, nx, ny, nz, out=out)
+    step()
+    torch.cuda.synchronize()
+    first = out.clone()
+    ms = _timed(step, steps, warmup)
+    n = nx * ny * nz
+    res = {"case": name, "points": n, "ms": ms, "gpoints_per_s": n / (ms * 1e-3) / 1e9,
+           "dram_gbs": 8.0 * n / (ms * 1e-3) / 1e9, "bytes_per_point": 8}
+    if check:
+        res["changed_after_repeat"] = int((out != first).sum())
+    return res
+
+
 def run_case(name: str, steps: int = 10, warmup: int = 3, error: bool = True,
              profile: bool = False, device=None) -> dict:
     c = parse_case(name)
+    if "NX" in c:
+        return run_jacobi(name, steps, warmup, error and not profile, device)
     if "NUM-OPTION" in c:
         return run_blackscholes(name, steps, warmup, error and not profile, device)
     device = device or torch.device("cuda", torch.cuda.current_device())

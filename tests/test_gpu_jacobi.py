@@ -69,3 +69,11 @@ def test_errors(hb):
     assert L.hbsg_jacobi(2, 4, None, a.data_ptr(), 4, 4, 4, None) == _lib.ERR_INVALID_ARG
     assert L.hbsg_jacobi(2, 4, None, None, 0, 4, 4, None) == _lib.OK
     assert L.hbsg_jacobi(2, 4, None, None, -1, 4, 4, None) == _lib.ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("case", ["nx_64__ny_8__nz_512", "nx_32__ny_8__nz_512",
+                                  "nx_512__ny_512__nz_512"])
+def test_sweep_named_case(case):
+    from hb_hammerbench_b200 import sweep
+    r = sweep.run_case(case, steps=2, warmup=1)
+    assert r["points"] > 0 and r["changed_after_repeat"] == 0

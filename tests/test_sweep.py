@@ -25,6 +25,11 @@ def test_blackscholes_names():
     assert c == {"NUM-OPTION": 10000000, "LAYOUT": "arrays"}
 
 
+def test_jacobi_names():
+    # apps/jacobi/tests.mk:1-2 registers nx_64__ny_8__nz_512 and nx_32__ny_8__nz_512
+    assert sweep.parse_case("nx_64__ny_8__nz_512") == {"NX": 64, "NY": 8, "NZ": 512}
+
+
 @pytest.mark.parametrize("bad", ["N_512__V_fp64", "NITER_2", "N__512", "SEED_1__V_ffma"])
 def test_bad_names(bad):
     with pytest.raises(ValueError):
