@@ -30,7 +30,7 @@ def test_reference_launches_exact(hb, oracle_mod, nx, ny, nz):
 
 
 @pytest.mark.parametrize("nx,ny,nz", [(1, 1, 1), (5, 3, 7), (33, 17, 65), (128, 40, 300),
-                                      (7, 129, 33)])
+                                      (7, 129, 33), (9, 5, 4), (3, 20, 132), (17, 3, 512)])
 @pytest.mark.parametrize("wide", [False, True])
 def test_random_grids_exact(hb, oracle_mod, nx, ny, nz, wide):
     rng = np.random.Generator(np.random.PCG64(nx * 1000 + ny * 10 + nz))
@@ -40,6 +40,23 @@ def test_random_grids_exact(hb, oracle_mod, nx, ny, nz, wide):
     for c0, c1 in ((2, 4), (-3, 7)):
         assert np.array_equal(_run(hb, a, nx, ny, nz, c0, c1),
                               oracle_mod.host_jacobi(a, nx, ny, nz, c0, c1))
+
+
+def test_vector_and_scalar_forms_agree(hb, oracle_mod):
+    """nz a multiple of 4 with 16-byte aligned grids takes the 4-wide form; the
+    same grid 4 bytes off alignment takes the scalar form; both exact."""
+    import torch
+    nx, ny, nz = 11, 9, 136
+    rng = np.random.Generator(np.random.PCG64(99))
+    a = rng.uniform(-1, 1, nx * ny * nz).astype(np.float32)
+    exp = oracle_mod.host_jacobi(a, nx, ny, nz)
+    buf = torch.zeros(2 * a.size + 8, device="cuda")
+    for off in (0, 1):
+        src = buf[off:off + a.size]
+        src.copy_(torch.from_numpy(a))
+        dst = buf[a.size + 4 + off:a.size + 4 + off + a.size]
+        got = hb.jacobi(src, nx, ny, nz, out=dst).cpu().numpy()
+        assert np.array_equal(got, exp), off
 
 
 def test_large_grid_exact_sampled(hb, oracle_mod):
