@@ -56,6 +56,34 @@ def test_noalloc_matches_workspace_entry_point_twice(variant):
         assert rel < (2.0 ** -16 if variant == "bf16x3" else 2e-6)
 
 
+@pytest.mark.parametrize("variant", ["bf16x6", "bf16x3"])
+def test_noalloc_tall_narrow_product(variant):
+    """A tall, narrow product, for which the library's own schedule splits B
+    in a pass of its own into the scratch and A inside the product kernel."""
+    import torch
+
+    import hb_hammerbench_b200 as hb
+    from hb_hammerbench_b200 import _lib
+    L = _lib.lib()
+    v = _lib.VARIANTS[variant]
+    m, n, k = 16384, 64, 2048
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for call, seed in enumerate((3, 4)):
+        A = _rand((m, k), seed)
+        B = _rand((k, n), seed + 100)
+        C = torch.full((m, n), float("nan"), device="cuda")
+        st = L.hbsg_gemm_noalloc(0, 0, m, n, k, _p(A), k, _p(B), n, _p(C), n, v, stream)
+        assert st == _lib.OK, (call, L.hbsg_strerror(st))
+        need = hb.gemm_workspace_size(m, n, k, variant)
+        ws = torch.empty(max(need, 256), dtype=torch.uint8, device="cuda")
+        C_ref = torch.empty((m, n), device="cuda")
+        st = L.hbsg_gemm_ex(0, 0, m, n, k, _p(A), k, _p(B), n, _p(C_ref), n, v, None,
+                            _p(ws), need, stream)
+        assert st == _lib.OK
+        torch.cuda.synchronize()
+        assert torch.equal(C, C_ref), call
+
+
 def test_noalloc_transposed_operands():
     import torch
 
