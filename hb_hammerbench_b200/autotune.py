@@ -201,7 +201,10 @@ def tune_grouped(As, Bs, variant: str = "bf16x6", steps: int = 3, store: bool = 
     from .sgemm import GroupedPlan, tiles
     fam = "ffma" if variant == "ffma" else "bf16"
     parts = 0 if fam == "ffma" else (3 if "x6" in variant else 2)
-    ids = [t["tile"] for t in tiles() if t["family"] == fam and t["parts"] == parts]
+    # grouped plans run every tile family except the A-in-TMEM fused tiles
+    # (fused tiles 128 rows high)
+    ids = [t["tile"] for t in tiles() if t["family"] == fam and t["parts"] == parts
+           and not (t["fused"] and t["bm"] == 128)]
     table = []
     for tile, raster in itertools.product(ids, (8, 16)):
         cfg = {"tile": tile, "raster_group": raster}
