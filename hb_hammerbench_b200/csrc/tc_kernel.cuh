@@ -263,7 +263,7 @@ struct TcRun {
 // Scaled forms apply 2^(row exponent + column exponent) first.
 template <int COLS, bool SCALED, int VW = 4>
 HBSG_DEV void store_rows_transposed(float* sum, const TileWork& w, int row0, int col0, int lane,
-                                    const int* wexp) {
+                                    const int* wexp, int row_end = 0x7fffffff) {
   static_assert(VW == 4, "16-byte chunks (float4 stores)");
   constexpr int NCH = 32 / VW;  // chunks per 32-column block = lanes per group
   if constexpr (SCALED) {
@@ -298,7 +298,7 @@ HBSG_DEV void store_rows_transposed(float* sum, const TileWork& w, int row0, int
 #pragma unroll
     for (int rho = 0; rho < NCH; ++rho) {
       const int r = rb + rho;
-      if (r >= w.M) continue;
+      if (r >= w.M || r >= row_end) continue;
       float* p = w.C + (long)r * w.ldc + c;
       const float* v = x + VW * rho;
       if (vec && c + VW - 1 < w.N) {
@@ -378,11 +378,12 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
   const unsigned long long lim = run.wait_limit_ns;
 
   // Next entry of the tile queue for a consumer (the MMA issuer, or lane 0 of
-  // an epilogue warp): {tile or -1, k-tiles, MMA width}; false on abort.
+  // an epilogue warp): {tile or -1, k-tiles, MMA width, valid rows}; false on
+  // abort.
   auto queue_take = [&](uint32_t& q, int4& e) -> bool {
     const int j = (int)(q % kTileQueue);
     if (!wait_bounded(&qfull[j], (q / kTileQueue) & 1, abort_flag, lim)) return false;
-    e = make_int4(qent[4 * j], qent[4 * j + 1], qent[4 * j + 2], 0);
+    e = make_int4(qent[4 * j], qent[4 * j + 1], qent[4 * j + 2], qent[4 * j + 3]);
     mbar_arrive(&qempty[j]);
     ++q;
     return true;
@@ -421,6 +422,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           qent[4 * j] = t < num_tiles ? t : -1;
           qent[4 * j + 1] = t < num_tiles ? w.KT : 0;
           qent[4 * j + 2] = nv;
+          qent[4 * j + 3] = t < num_tiles ? min(kBM, w.M - w.m0) : 0;
           mbar_arrive(&qfull[j]);
           ++q;
         }
@@ -502,7 +504,7 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
         if (t < num_tiles) w = tiles.get(t);
       }
       for (;;) {
-        int KT, nv;
+        int KT, nv, mv;
         if constexpr (Tiles::kQueue) {
           int4 e = make_int4(-1, 0, 0, 0);
           int got = 1;
@@ -511,18 +513,24 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           if (tile < 0) break;  // -1: end of the sequence; -2: abort
           KT = __shfl_sync(0xffffffffu, e.y, 0);
           nv = __shfl_sync(0xffffffffu, e.z, 0);
+          mv = __shfl_sync(0xffffffffu, e.w, 0);
         } else {
           if (t >= num_tiles) break;
           TileWork nx = w;
           if (t + (int)gridDim.x < num_tiles) nx = tiles.get(t + gridDim.x);
           KT = w.KT;
           nv = min(BN, w.N - w.n0);
+          mv = min(kBM, w.M - w.m0);
           w = nx;
           t += gridDim.x;
         }
-        // MMA width trimmed to the tile's valid columns (multiple of 16): the
-        // last column tile of a problem does no tensor work on padding.
-        const uint32_t idesc = f16_idesc(kBM, nv >= BN ? BN : ((nv + 15) & ~15));
+        // MMA width trimmed to the tile's valid columns (multiple of 16), and
+        // its height to 64 when the tile holds at most 64 valid rows: the
+        // last row and column tiles of a problem do less tensor work on
+        // padding. (An M = 64 accumulator holds row r in lane
+        // 32 (r / 16) + r % 16; the epilogue reads it so.)
+        const uint32_t idesc =
+            f16_idesc(mv <= 64 ? 64 : kBM, nv >= BN ? BN : ((nv + 15) & ~15));
         const int nchunks = (KT + run.chunk_ktiles - 1) / run.chunk_ktiles;
         int kt = 0;
         for (int c = 0; c < nchunks && ok; ++c, ++ch) {
@@ -624,7 +632,13 @@ __device__ __forceinline__ void tc_body(const Tiles& tiles, const TcRun& run) {
           wexp[i] = pow2_exp_of_bits(w.colmax[min(col0 + i, w.N - 1)]);
         __syncwarp();
       }
-      store_rows_transposed<COLS, SCALED>(sum, w, w.m0 + 32 * q, col0, lane, wexp);
+      // an M = 64 accumulator (tiles with at most 64 valid rows) holds rows
+      // 16 q .. 16 q + 15 in lanes 32 q .. 32 q + 15 of the warp's quadrant
+      if (w.M - w.m0 <= 64)
+        store_rows_transposed<COLS, SCALED>(sum, w, w.m0 + 16 * q, col0, lane, wexp,
+                                            w.m0 + 16 * q + 16);
+      else
+        store_rows_transposed<COLS, SCALED>(sum, w, w.m0 + 32 * q, col0, lane, wexp);
     }
   }
 
