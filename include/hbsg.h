@@ -82,8 +82,11 @@ typedef struct hbsg_tile_info {
     int smem_bytes;    /* dynamic shared memory per CTA */
     int parts;         /* split-BF16 family: BF16 parts per operand (3 -> BF16X6 forms,
                           2 -> BF16X3 forms); 0 for the FFMA family */
-    int fused;         /* 1: the FP32 -> BF16 split runs inside the product kernel (no
-                          split pass, no parts in the workspace; row-major operands only) */
+    int fused;         /* 1: the FP32 -> BF16 split runs inside the product kernel
+                          (row-major operands with 16-byte aligned rows only): for both
+                          operands on the 256-row CTA-pair tiles (no parts in the
+                          workspace); for A on the 128-row tiles, which keep A's parts in
+                          tensor memory and split B in a pass into the workspace */
 } hbsg_tile_info;
 
 /* ---------------------------------------------------------------------------
