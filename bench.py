@@ -506,7 +506,7 @@ def _ffma_roofline(kernel_ms: float, flops: float, fp32: dict, n: int) -> dict:
                           "on this device in this run"}
 
 
-# BASELINE configurations measured beside the headline: the uneven grouped
+# Workloads measured beside the headline: the uneven grouped
 # batch (512 problems) and the two awkward shapes, each one named case of the
 # sweep driver (seeded device inputs larger than L2; error vs FP64).
 LEGS = [

@@ -5,7 +5,7 @@ Bars:
     for every variant (small integers split exactly and sum exactly);
   - the split pre-pass: bit-exact against the oracle's split (oracle.c);
   - floating point: error vs the FP64 product no worse than the FFMA kernel's
-    for the 6-product forms at K >= 512, and within
+    for the 6-product forms at K >= 512 (the precision form's error bar), and within
     stated bounds otherwise.
 """
 import ctypes

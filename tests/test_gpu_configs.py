@@ -15,7 +15,7 @@ every split-BF16 test compares with equals the oracle's FP64 product (oracle.c,
 sequential double accumulation) on sampled rows.
 
 Bars: the 6-product forms are no worse than the FFMA kernel against FP64 (the
-north-star tolerance); the 3-product forms stay within 2^-16 relative
+precision form's error bar); the 3-product forms stay within 2^-16 relative
 Frobenius error (their 2-part split holds ~16 bits).
 """
 import numpy as np
