@@ -14,8 +14,9 @@ KEY_value fields. Recognised keys:
                              run as one grouped plan (CUDA-graph replay)
   V_<variant>                ffma | bf16x3 | bf16x6 | bf16x3_scaled | bf16x6_scaled
   DIST_<d>                   uniform (U[-1,1), default) | wide (sign * 2^u, u ~ U[-20,20])
-  SPLITK_<s> / TILE_<t> / CHUNK_<c>
-                             explicit schedule (hbsg_config.split_k / .tile / .chunk_k)
+  SPLITK_<s> / TILE_<t> / CHUNK_<c> / RASTER_<r>
+                             explicit schedule (hbsg_config.split_k / .tile / .chunk_k /
+                             .raster_group)
   num-option_<n>             Black-Scholes (apps/blackscholes/tests.mk:1): n seeded
                              synthetic option records priced in place
   LAYOUT_<l>                 Black-Scholes layout: records (default) | arrays
@@ -101,6 +102,8 @@ def _config(c: dict):
         cfg["tile"] = c["TILE"]
     if "CHUNK" in c:
         cfg["chunk_k"] = c["CHUNK"]
+    if "RASTER" in c:
+        cfg["raster_group"] = c["RASTER"]
     return cfg or None
 
 

@@ -16,6 +16,9 @@ def test_general_and_grouped_names():
     assert c == {"M": 256, "N": 256, "K": 1048576, "V": "bf16x6", "SPLITK": 74}
     g = sweep.parse_case("GROUPED_512__SEED_0__V_ffma")
     assert g["GROUPED"] == 512 and g["SEED"] == 0
+    s = sweep.parse_case("M_8192__N_8192__K_8192__V_bf16x6__TILE_10__SPLITK_0__CHUNK_64__RASTER_16")
+    assert sweep._config(s) == {"split_k": 0, "tile": 10, "chunk_k": 64, "raster_group": 16}
+    assert sweep._config(sweep.parse_case("N_512__NITER_2")) is None
 
 
 def test_blackscholes_names():
